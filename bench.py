@@ -1,0 +1,312 @@
+"""Benchmark of the witness search: verified witnesses/s on S_16, bound 9.
+
+Workload (the full-size decision search): 2^20 seeded permutations of S_16
+(nibble-packed), half uniform (Fisher-Yates) and half the reverse permutation
+composed with 1-4 random block transpositions; decide whether each sorts
+within 9 moves in the reference's move space and emit a witness.  A step is
+one pass of the engine over the whole batch followed by the device replay of
+every witness; `value` counts replay-verified witnesses per second with the
+instances already resident in HBM.  `e2e` is the same metric through the
+public host-buffer call (td_search_batch with TD_FLAG_VERIFY): host-to-device
+copy of the instances, search, replay and device-to-host copy of the results.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With --impl reference the CPU restatement of the reference search (the
+reference ships no CPU search of its own) is timed on all host cores on a
+bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+COUNT = 1 << 20
+SEED = 2
+MAX_MOVES = 9
+METRIC = "verified witnesses/s (S_16, d<=9)"
+UNIT = "witnesses/s"
+WORKLOAD = "full-size decision search: 2^20 S_16 perms, 50% uniform / 50% reverse o 1-4 transpositions, d<=9"
+# warp instructions executed per node expansion by the search kernel at N=17,
+# from the ncu capture summarised in profiles/td_persistent_kernel_s16.md
+INST_PER_EXPANSION = None
+
+
+def rank_info():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_instances(td, rank):
+    perms, n = td.synth_perms(SEED ^ (rank << 40), COUNT, 16, 16, 50, 1, 4)
+    return td.prepare_perms(perms, n, MAX_MOVES), perms, n
+
+
+def cpu_baseline(seconds_target=15.0, sample=96):
+    """The oracle (CPU restatement of the reference search, its single-queue
+    order) on all host cores, on a bounded sample of the workload."""
+    from oracle import oracle as O
+    import td16_b200 as td
+    perms, n = td.synth_perms(SEED, sample, 16, 16, 50, 1, 4)
+    c = len(n)
+    beta = np.zeros((c, 17), np.uint8)
+    omega = np.zeros((c, 17), np.uint8)
+    init = np.zeros(c, np.int32)
+    for i in range(c):
+        b, o, e = O.perm_to_pair(perms[i, :16].tolist())
+        beta[i], omega[i], init[i] = b, o, e
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    st, dep, mv, ex = O.search_batch(beta, omega, np.full(c, 17), init, np.zeros(c), np.full(c, MAX_MOVES),
+                                     np.ones(c), cores)
+    dt = time.perf_counter() - t0
+    # every oracle witness is replayed by the oracle's checker before it counts
+    verified = 0
+    for i in np.nonzero(st == 1)[0]:
+        moves = [(int(m) & 31, (int(m) >> 5) & 31, (int(m) >> 10) & 31) for m in mv[i][: dep[i]]]
+        abc = O.positions_to_symbols(beta[i].tolist(), moves)
+        verified += O.validate(beta[i].tolist(), omega[i].tolist(), abc, MAX_MOVES) is None
+    return {"value": verified / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"first {c} instances of the workload (seed {SEED}), {dt:.1f} s on {cores} threads",
+            "expansions_per_s": float(ex.sum()) / dt, "seconds": dt}
+
+
+def run_reference(args):
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return
+    steps = []
+    for _ in range(args.warmup):
+        cpu_baseline(sample=16)
+    res = None
+    for _ in range(args.steps):
+        res = cpu_baseline(sample=48)
+        steps.append(res)
+    value = float(np.mean([s["value"] for s in steps]))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": float(np.mean([s["seconds"] for s in steps]) * 1e3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/u64 integer",
+            "data": "synthetic (seeded)", "config": {"workload": WORKLOAD, "count": COUNT, "seed": SEED,
+                                                     "max_moves": MAX_MOVES, "l2": "n/a (CPU)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": res["cores"], "kind": "port",
+                             "sample": res["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_engine(args):
+    import torch
+    import td16_b200 as td
+    from td16_b200 import _lib
+
+    rank, world, local = rank_info()
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    td.init_slots(1, [local], 256 << 20)
+    stream_ptr = _lib.lib().td_slot_stream(0)
+    stream = torch.cuda.ExternalStream(stream_ptr, device=dev)
+
+    inst, perms, n = make_instances(td, rank)
+    count = len(inst)
+    d_in = torch.from_numpy(inst.view(np.uint8).copy()).to(dev)
+    d_out = torch.zeros(count * 32, dtype=torch.uint8, device=dev)
+    d_ok = torch.zeros(count, dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # larger than the 126 MB L2
+
+    def step(flags):
+        _lib.search_batch_device(0, count, d_in.data_ptr(), d_out.data_ptr(), flags, 0, stream_ptr)
+        _lib.validate_batch_device(count, d_in.data_ptr(), d_out.data_ptr(), d_ok.data_ptr(), stream_ptr)
+
+    for _ in range(args.warmup):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        step(0)
+    torch.cuda.synchronize()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    verified, expansions, found, not_found, errors = 0, 0, 0, 0, 0
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            ev[k][0].record(stream)
+            step(0)
+            ev[k][1].record(stream)
+            torch.cuda.synchronize()
+            res = d_out.cpu().numpy().view(_lib.RESULT_DTYPE)
+            ok = d_ok.cpu().numpy()
+            verified += int(ok.sum())
+            expansions += int(res["expansions"].astype(np.int64).sum())
+            found += int((res["status"] == 1).sum())
+            not_found += int((res["status"] == 0).sum())
+            errors += int((res["status"] < 0).sum())
+    torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_s = sum(step_ms) / 1e3
+    if dist:
+        t = torch.tensor([total_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_s = float(t.item())
+        agg = torch.tensor([verified, expansions, found, not_found, errors], device=dev, dtype=torch.float64)
+        dist.all_reduce(agg)
+        verified, expansions, found, not_found, errors = [int(v) for v in agg.tolist()]
+    value = verified / total_s
+
+    # end to end through the public host-buffer API
+    host_in = inst.copy()
+    e2e_s, e2e_verified = 0.0, 0
+    for k in range(max(1, min(args.steps, 3))):
+        t0 = time.perf_counter()
+        res_h, st = td.search_batch(0, host_in, _lib.FLAG_VERIFY)
+        e2e_s += time.perf_counter() - t0
+        e2e_verified += int((res_h["status"] == 1).sum())
+    e2e_steps = max(1, min(args.steps, 3))
+
+    # the plain one-launch-per-batch form on the same GPU
+    pe = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    with torch.cuda.stream(stream):
+        flush.zero_()
+    pe[0].record(stream)
+    step(_lib.FLAG_PLAIN)
+    pe[1].record(stream)
+    torch.cuda.synchronize()
+    plain_ms = pe[0].elapsed_time(pe[1])
+    plain_verified = int(d_ok.sum().item())
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    # roofline: integer issue of the search kernel against the measured ALU peak
+    import ctypes as C
+    peak, pk_ms = C.c_double(), C.c_double()
+    err = C.create_string_buffer(256)
+    _lib.lib().td_int_issue_peak.argtypes = [C.c_int, C.c_float, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                             C.c_char_p, C.c_size_t]
+    _lib.lib().td_int_issue_peak(local, 200.0, C.byref(peak), C.byref(pk_ms), err, 256)
+    per_step_exp = expansions / max(1, args.steps) / world
+    mean_ms = float(np.mean(step_ms))
+    nodes_per_s = per_step_exp / (mean_ms / 1e3)
+    triples_per_s = nodes_per_s * 680
+    roofline = {"bound": "int-issue", "unit": "Gwarp-inst/s", "peak": peak.value / 1e9,
+                "peak_source": "measured live: LOP3 chains on every SM (td_int_issue_peak)",
+                "achieved": None, "frac": None, "traffic": None,
+                "nodes_per_s": nodes_per_s, "triples_per_s": triples_per_s}
+    if INST_PER_EXPANSION:
+        ach = nodes_per_s * INST_PER_EXPANSION
+        roofline["achieved"] = ach / 1e9
+        roofline["frac"] = ach / peak.value
+
+    cpu = cpu_baseline() if world == 1 else None
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": mean_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8/u64 integer", "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "count_per_gpu": count, "seed": SEED, "max_moves": MAX_MOVES,
+                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
+        "nodes_per_s": nodes_per_s, "triples_per_s": triples_per_s,
+        "found": found, "not_found": not_found, "errors": errors, "verified": verified,
+        "plain_one_launch": {"value": plain_verified / (plain_ms / 1e3), "ms": plain_ms},
+        "e2e": {"value": e2e_verified / e2e_s, "unit": UNIT, "h2d_bytes_per_step": count * 16,
+                "d2h_bytes_per_step": count * 32, "ms_per_step": e2e_s / e2e_steps * 1e3},
+        "gpu_launches": args.steps * 2,
+        "roofline": roofline,
+        "clocks": clocks.summary(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_engine(args)
+
+
+if __name__ == "__main__":
+    main()

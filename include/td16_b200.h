@@ -1,0 +1,171 @@
+/*
+ * td16_b200.h -- C ABI of the B200 witness-search engine (libtd16b200.so).
+ *
+ * Drop-in for the td16 emitter's native boundary.  The reference binds two
+ * JNI entry points of class br.unb.cic.tdp.base.GPUSortingSearch
+ * (emitter/src/main/java/br/unb/cic/tdp/base/GPUSortingSearch.java:115-117):
+ *   initSlots(int totalSlots, int[] devices, long queueBytesBudget)
+ *   searchForSortingSeq(byte[] beta, byte[] omega, int initialEvenCycles,
+ *                       float minRate, int maxMoves, boolean fullSorting, int slot)
+ * td_init_slots and td_search replace them one for one; the batch, serving
+ * and codec entry points are additions.  All buffers are plain host or device
+ * pointers; no entry point takes or returns a C++ or framework type.
+ */
+#ifndef TD16_B200_H
+#define TD16_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (return values of the entry points) ------------------ */
+#define TD_OK 0            /* search ran and found a witness               */
+#define TD_NOT_FOUND 1     /* search ran to exhaustion without a witness   */
+#define TD_OVERFLOW 2      /* work budget exhausted before a verdict
+                              (the reference's "GPU sorting search queue
+                              overflow", sorting_search.cu:960-962)         */
+#define TD_CUDA_ERROR 3    /* a CUDA call failed; message in err           */
+#define TD_INVALID_ARG 4   /* rejected input; message in err               */
+#define TD_TIMEOUT 5       /* deadline or abort request reached            */
+
+/* ---- per-instance records ------------------------------------------------ */
+
+/* One search in pinned form (16 bytes).  Build it with td_prepare_pairs or
+ * td_prepare_perms; the layout is documented for callers that keep
+ * instances resident on the device. */
+typedef struct td_instance {
+    uint64_t perm;      /* nibble m = L[m] (m < N-1); nibble m >= N-1 holds m */
+    float min_rate;     /* minRate (f32), as passed by the reference's callers */
+    uint8_t n_symbols;  /* N = length of beta, <= 17 */
+    uint8_t offset;     /* pinned position of the caller's beta[0] */
+    uint8_t max_moves;  /* 1..9 */
+    uint8_t packed;     /* bits 0-4 initialEvenCycles, bit 7 fullSorting */
+} td_instance;
+
+/* One result (32 bytes).  moves[] are position triples into the caller's
+ * evolving beta array packed as i | j<<5 | k<<10, the reference's PackedMove
+ * (core/common.cuh:42-54). */
+typedef struct td_result {
+    int32_t status;       /* 1 found, 0 not found, <0 error (-2 budget, -4 argument, -5 timeout) */
+    int32_t depth;        /* number of moves */
+    uint16_t moves[9];
+    uint16_t reserved;
+    uint32_t expansions;  /* nodes whose children were evaluated */
+} td_result;
+
+/* batch flags */
+#define TD_FLAG_ORDERED 1u     /* reference single-queue move order: witness
+                                  identical to the reference run with one queue */
+#define TD_FLAG_PLAIN 2u       /* one launch, one warp per instance, no work
+                                  distribution (the baseline form) */
+#define TD_FLAG_VERIFY 4u      /* replay every witness on the device after the
+                                  search; a witness that fails the replay gets
+                                  status -6 */
+
+typedef struct td_batch_stats {
+    uint64_t expansions;   /* total nodes expanded */
+    uint64_t found;        /* instances with a witness */
+    uint64_t not_found;    /* instances exhausted */
+    uint64_t errors;       /* instances with status < 0 */
+    float kernel_ms;       /* device time of the search launch(es) */
+} td_batch_stats;
+
+/* ---- slots: the reference's JNI boundary --------------------------------- */
+
+/* Replaces Java_br_unb_cic_tdp_base_GPUSortingSearch_initSlots
+ * (emitter/src/native/jni/jni_sorter.cu:24-47 -> slot_manager.cu:44-128).
+ * Slot s runs on devices[s % device_count], each with its own stream,
+ * completion event and `queue_bytes_budget` bytes of device scratch.  Fails
+ * with TD_INVALID_ARG on an empty, duplicate or out-of-range device list,
+ * total_slots <= 0 or a zero budget, and when a device has less free memory
+ * than budget x its slots.  Re-initialises: previous slots are destroyed. */
+int td_init_slots(int total_slots, const int *devices, int device_count,
+                  uint64_t queue_bytes_budget, char *err, size_t errlen);
+
+/* Replaces Java_br_unb_cic_tdp_base_GPUSortingSearch_searchForSortingSeq
+ * (jni_sorter.cu:49-117 -> sorting_search.cu:811-972).  beta and omega hold
+ * n unsigned bytes each (n <= 17), 1 <= max_moves <= 9.  Blocking; one caller
+ * per slot at a time, different slots run concurrently.  On TD_OK writes
+ * *out_depth position triples (i,j,k), i<j<k, to out_ijk[3*d..3*d+2]; on
+ * TD_NOT_FOUND *out_depth = 0 (also for n < 3). */
+int td_search(int slot, const uint8_t *beta, const uint8_t *omega, int n,
+              int initial_even_cycles, float min_rate, int max_moves,
+              int full_sorting, int16_t *out_ijk, int *out_depth, char *err,
+              size_t errlen);
+
+/* Same search with the reference's single-queue move order (its
+ * performGpuSortingSearch with maxWarps = 1, sorting_search.cu:842): the
+ * witness is the one that order finds first. */
+int td_search_ordered(int slot, const uint8_t *beta, const uint8_t *omega, int n,
+                      int initial_even_cycles, float min_rate, int max_moves,
+                      int full_sorting, int16_t *out_ijk, int *out_depth,
+                      char *err, size_t errlen);
+
+int td_slot_count(void);
+int td_slot_device(int slot);           /* -1 for an invalid slot */
+void *td_slot_stream(int slot);         /* cudaStream_t of the slot */
+int td_destroy(void);                   /* releases every slot */
+
+/* ---- instance preparation (host, no GPU needed) -------------------------- */
+
+/* count pairs, beta/omega with a stride of 17 bytes per instance.  Returns
+ * TD_OK or TD_INVALID_ARG (index of the first bad instance in *bad). */
+int td_prepare_pairs(int count, const uint8_t *beta, const uint8_t *omega,
+                     const uint8_t *n, const int32_t *initial_even_cycles,
+                     const float *min_rate, const int32_t *max_moves,
+                     const uint8_t *full_sorting, td_instance *out, int *bad);
+
+/* count permutations of S_n (int8, stride 16): the reference pair over n+1
+ * symbols with beta = (0 1 ... n) and rho = (0, pi0+1, ..., pi_{n-1}+1);
+ * initialEvenCycles is computed. */
+int td_prepare_perms(int count, const int8_t *perms, const uint8_t *n,
+                     const int32_t *max_moves, float min_rate, int full_sorting,
+                     td_instance *out, int *bad);
+
+/* Seeded synthetic permutations: instance i uses splitmix64 seeded with
+ * seed ^ i; n uniform in [n_min, n_max]; with probability hard_pct/100 the
+ * reverse permutation composed with hard_min..hard_max uniform block
+ * transpositions, else Fisher-Yates uniform.  perms int8 stride 16. */
+int td_synth_perms(uint64_t seed, int count, int n_min, int n_max, int hard_pct,
+                   int hard_min, int hard_max, int8_t *perms, uint8_t *n);
+
+/* ---- batch search -------------------------------------------------------- */
+
+/* Host buffers in and out; copies, launches and waits on the slot's stream. */
+int td_search_batch(int slot, int count, const td_instance *instances,
+                    td_result *results, unsigned flags,
+                    uint64_t max_expansions, td_batch_stats *stats, char *err,
+                    size_t errlen);
+
+/* Device buffers; enqueues on `stream` (a cudaStream_t, or NULL for the
+ * slot's stream) and returns without waiting. */
+int td_search_batch_device(int slot, int count, const td_instance *d_instances,
+                           td_result *d_results, unsigned flags,
+                           uint64_t max_expansions, void *stream, char *err,
+                           size_t errlen);
+
+/* Replays witnesses on the device with the reference checker's rules
+ * (CertificateValidator.java:14-50): d_ok[i] = 1 when results[i] is a found
+ * witness that sorts instance i within its max_moves, 0 otherwise. */
+int td_validate_batch_device(int count, const td_instance *d_instances,
+                             const td_result *d_results, uint8_t *d_ok,
+                             void *stream, char *err, size_t errlen);
+
+/* Measures the device's ALU-pipe integer issue rate (warp instructions per
+ * second of independent LOP3 chains at full occupancy), the denominator of the
+ * search kernel's roofline. */
+int td_int_issue_peak(int device, float target_ms, double *warp_inst_per_s,
+                      double *ms, char *err, size_t errlen);
+
+/* Position triples -> symbol triples on a copy of beta
+ * (GPUSortingSearch.java:229-238). */
+void td_positions_to_symbols(const uint8_t *beta, int n, const int16_t *ijk,
+                             int depth, uint8_t *out_abc);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

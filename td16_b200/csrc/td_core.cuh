@@ -1,0 +1,285 @@
+// td_core.cuh -- definitions shared by the sm_100a kernels and the host side of
+// the witness-search engine.  Everything here is plain integer arithmetic that
+// compiles for both host and device (__host__ __device__), so the host can
+// prepare instances and tests can exercise the same logic without a GPU.
+//
+// Vocabulary (reference: emitter/src/native/backtracking/sorting_search.cu):
+//   N      number of symbols (n + 1 for a permutation of S_n), N <= 17
+//   beta   the current N-cycle, written as an array that starts at betaStart
+//   omega  the algebraic permutation; rho = omega . beta stays fixed
+//   move   a position triple i < j < k into the beta array; it swaps the blocks
+//          [i,j) and [j,k) and sets omega <- omega . (a b c)^-1 with
+//          (a,b,c) = (beta[i], beta[j], beta[k])
+//
+// Engine state ("pinned" form).  Relabel the symbols so that rho becomes
+// x -> x+1 (mod N) and write beta as the cyclic sequence B that starts at
+// symbol 0.  The remaining n = N-1 entries L[m] = B[m+1]-1 form a linear
+// permutation of 0..n-1 that fits 4-bit nibbles of one uint64.  The caller's
+// array start (betaStart) is tracked as `off`, the position in B of the
+// caller's beta[0]; caller position p is pinned position (p + off) mod N.
+#pragma once
+
+#include <math.h>
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define TD_HD __host__ __device__ __forceinline__
+#else
+#define TD_HD inline
+#endif
+
+#define TD_MAX_N 17      // symbols (core/common.cuh:14-16)
+#define TD_MAX_DEPTH 9   // moves (core/common.cuh:10-12)
+#define TD_MAX_TRIPLES 680
+#define TD_MAX_STEPS 22  // ceil(680 / 32)
+#define TD_PT_STRIDE 32  // pair table row stride (bytes)
+
+// ---- C-ABI records (mirrored in include/td16_b200.h) ----------------------
+
+// One search request in pinned form: 16 bytes.
+struct td_instance {
+    uint64_t perm;      // nibble m = L[m] for m < N-1; nibbles m >= N-1 hold m
+    float min_rate;     // the reference's minRate (f32)
+    uint8_t n_symbols;  // N
+    uint8_t offset;     // pinned position of the caller's beta[0]
+    uint8_t max_moves;  // 1..9
+    uint8_t packed;     // bits 0-4: initialEvenCycles, bit 7: fullSorting
+};
+
+// One search result: 32 bytes.
+struct td_result {
+    int32_t status;      // TD_FOUND / TD_NOT_FOUND / error code (<0)
+    int32_t depth;       // witness length
+    uint16_t moves[TD_MAX_DEPTH];  // caller positions, i | j<<5 | k<<10
+    uint16_t reserved;
+    uint32_t expansions; // nodes whose children were evaluated (saturating)
+};
+
+#define TD_FOUND 1
+#define TD_NOT_FOUND 0
+#define TD_ERR_ARG (-4)
+#define TD_ERR_BUDGET (-2)
+#define TD_ERR_TIMEOUT (-5)
+
+#define TD_FLAG_ORDERED 1u  // reproduce the reference's single-queue move order
+
+// ---- small helpers ---------------------------------------------------------
+
+TD_HD int td_triple_count(int n) { return n < 3 ? 0 : n * (n - 1) * (n - 2) / 6; }
+
+TD_HD uint16_t td_pack_move(int i, int j, int k) {
+    return (uint16_t)((i & 31) | ((j & 31) << 5) | ((k & 31) << 10));
+}
+
+TD_HD uint32_t td_nib(uint64_t L, int m) { return (uint32_t)(L >> (4 * m)) & 15u; }
+
+TD_HD uint64_t td_low_nibbles(int count) {  // mask of the lowest `count` nibbles
+    return count >= 16 ? ~0ull : ((1ull << (4 * count)) - 1ull);
+}
+
+TD_HD int td_inst_init(const td_instance &x) { return x.packed & 31; }
+TD_HD int td_inst_full(const td_instance &x) { return (x.packed >> 7) & 1; }
+
+// Apply the caller-position move (i,j,k) to the pinned state (L, off).
+// The three cut points are pinned positions P,Q,R in cyclic order; rotated so
+// that the smallest comes first they give (p1,p2,p3).  A block swap of the
+// cyclic sequence is the same cycle whichever arc the array starts in, so in
+// pinned form it is the linear transposition (x,y,z) = (p1-1,p2-1,p3-1), or
+// (p2-1,p3-1,n) when p1 == 0.  The caller's array start moves to beta[j] when
+// i == 0 (sorting_search.cu:450-452, 623-625).
+TD_HD void td_apply_move(uint64_t L, int off, int N, int i, int j, int k,
+                         uint64_t *outL, int *outOff) {
+    const int n = N - 1;
+    int P = i + off, Q = j + off, R = k + off;
+    P -= (P >= N) ? N : 0;
+    Q -= (Q >= N) ? N : 0;
+    R -= (R >= N) ? N : 0;
+    int p1, p2, p3;
+    if (P < Q && Q < R) { p1 = P; p2 = Q; p3 = R; }
+    else if (Q < R && R < P) { p1 = Q; p2 = R; p3 = P; }
+    else { p1 = R; p2 = P; p3 = Q; }
+    int x, y, z;
+    if (p1 == 0) { x = p2 - 1; y = p3 - 1; z = n; }
+    else { x = p1 - 1; y = p2 - 1; z = p3 - 1; }
+    const int a = y - x, b = z - y;  // lengths of the swapped blocks
+    const uint64_t keep = (L & td_low_nibbles(x)) | (L & ~td_low_nibbles(z));
+    const uint64_t blockA = (L >> (4 * x)) & td_low_nibbles(a);
+    const uint64_t blockB = (L >> (4 * y)) & td_low_nibbles(b);
+    *outL = keep | (blockB << (4 * x)) | (blockA << (4 * (x + b)));
+    // new start of the caller's array, followed through the swap
+    int S = (i == 0) ? Q : off;
+    if (S != 0) {
+        int e = S - 1;
+        if (e >= x && e < y) e += b;
+        else if (e >= y && e < z) e -= a;
+        S = e + 1;
+    }
+    *outOff = S;
+}
+
+// ---- triple classification -------------------------------------------------
+//
+// For a node, every ordered pair (p,q) of caller positions gets a 4-bit entry
+//   bit0 S: the symbols at p and q lie in the same omega cycle
+//   bit1 P: parity of the walk p -> q along omega (only when S)
+//   bit2 G: dist(p) > dist(q) when S, where dist is the number of omega steps
+//           to the cycle's smallest position; when !S: p's cycle is a fixed point
+//   bit3 O: p's cycle has odd length
+// A triple (i,j,k) reads entries (i,j), (j,k), (k,i) and forms a 12-bit index
+// into a table that restates delta_even_cycles (sorting_search.cu:240-332) and
+// the move filter (:375-380, :607-610).  Table values: 0 = filtered out,
+// 4 = odd-cycle change 0, 12 = change +2 (multiples of 4 so the value is the
+// shift into the per-node outcome word).
+
+#define TD_CLASS_SKIP 0
+#define TD_CLASS_ZERO 4
+#define TD_CLASS_PLUS2 12
+
+TD_HD int td_class_of_index(int idx) {
+    const int S1 = idx & 1, P1 = (idx >> 1) & 1, G1 = (idx >> 2) & 1, O1 = (idx >> 3) & 1;  // (a,b)
+    const int S2 = (idx >> 4) & 1, P2 = (idx >> 5) & 1, G2 = (idx >> 6) & 1, O2 = (idx >> 7) & 1;  // (b,c)
+    const int S3 = (idx >> 8) & 1, P3 = (idx >> 9) & 1, G3 = (idx >> 10) & 1, O3 = (idx >> 11) & 1;  // (c,a)
+    int delta;
+    if (S1 && S2 && S3) {
+        // one cycle: split in three when the omega order is a -> b -> c
+        if (O1 != O2 || O2 != O3) return TD_CLASS_SKIP;  // inconsistent
+        if (G1 + G2 + G3 != 2) return TD_CLASS_ZERO;
+        delta = P1 + P2 + P3 - O1;
+    } else if (S1 + S2 + S3 == 1) {
+        int o1, o2, s, lone_fixed;
+        if (S1) { o1 = O1; o2 = O3; s = P1; lone_fixed = G3; }       // {a,b}, c apart
+        else if (S2) { o1 = O2; o2 = O1; s = P2; lone_fixed = G1; }  // {b,c}, a apart
+        else { o1 = O3; o2 = O2; s = P3; lone_fixed = G2; }          // {c,a}, b apart
+        if (lone_fixed) return TD_CLASS_SKIP;
+        delta = s + (o1 ^ s ^ o2) - o1 - o2;
+    } else {
+        return TD_CLASS_SKIP;  // three cycles (or a fixed point alone)
+    }
+    if (delta == 2) return TD_CLASS_PLUS2;
+    if (delta == 0) return TD_CLASS_ZERO;
+    return TD_CLASS_SKIP;
+}
+
+// Per-position cycle descriptor: leader (smallest pinned position of the
+// cycle), dist (omega steps to the leader), len (cycle length).
+TD_HD uint32_t td_pair_entry(int leader_p, int dist_p, int len_p, int leader_q,
+                             int dist_q) {
+    const int S = leader_p == leader_q;
+    int P = 0, G;
+    if (S) {
+        int w = dist_p - dist_q;
+        if (w < 0) w += len_p;
+        P = w & 1;
+        G = dist_p > dist_q;
+    } else {
+        G = len_p == 1;
+    }
+    return (uint32_t)(S | (P << 1) | (G << 2) | ((len_p & 1) << 3));
+}
+
+// ---- acceptance and pruning masks ------------------------------------------
+//
+// satisfies_rate and can_still_reach (sorting_search.cu:336-373) depend only on
+// (oddCycles, depth); for each depth they become a bitmask over oddCycles.
+// The f32 operations are the reference's, in the same order.
+
+TD_HD int td_accepts(int N, int init, float min_rate, int full, int odd, int depth) {
+    if (depth <= 0) return 0;
+    if (full && odd != N) return 0;
+    const int gained = odd - init;
+    const float ratio = (float)gained / (float)depth;
+    return gained > 0 && ratio >= min_rate;
+}
+
+TD_HD int td_can_reach(int N, int init, float min_rate, int max_depth, int full,
+                       int odd, int depth) {
+    const int missing = N - odd;
+    if (full) return depth + (missing + 1) / 2 <= max_depth;
+    const int gained = odd - init;
+    const int left = max_depth - depth;
+    const int required = (int)floorf(min_rate * (float)max_depth);
+    if (gained + 2 * left < required) return 0;
+    const int best_depth = depth + (missing + 1) / 2;
+    if (best_depth > 0) {
+        const float best = (float)(gained + missing) / (float)best_depth;
+        if (best < min_rate) return 0;
+    }
+    return 1;
+}
+
+// ---- instance preparation (host side) --------------------------------------
+
+// Odd-length cycles of omega, fixed points included (sorting_search.cu:211-226).
+TD_HD int td_count_odd_cycles(const uint8_t *omega, int N) {
+    uint32_t seen = 0;
+    int odd = 0;
+    for (int s = 0; s < N; ++s) {
+        if (seen & (1u << s)) continue;
+        int len = 0, x = s;
+        do { seen |= 1u << x; ++len; x = omega[x]; } while (x != s);
+        odd += len & 1;
+    }
+    return odd;
+}
+
+// Caller pair (beta array, omega one-line) -> pinned instance.  Returns 0, or
+// TD_ERR_ARG when the sizes are out of range, an array is not a permutation of
+// 0..N-1, or rho = omega . beta is not an N-cycle (the reference's callers only
+// pass pairs whose product is an N-cycle, CyclicTargetPair.java:39-45).
+TD_HD int td_prepare_pair(const uint8_t *beta, const uint8_t *omega, int N, int init,
+                          float min_rate, int max_moves, int full, td_instance *out) {
+    if (N < 0 || N > TD_MAX_N) return TD_ERR_ARG;
+    if (max_moves <= 0 || max_moves > TD_MAX_DEPTH) return TD_ERR_ARG;
+    if (init < 0 || init > 31) return TD_ERR_ARG;
+    uint64_t L = 0;
+    for (int m = 0; m < 16; ++m) L |= (uint64_t)m << (4 * m);
+    if (N >= 1) {
+        uint32_t seen_b = 0, seen_o = 0;
+        for (int x = 0; x < N; ++x) {
+            if (beta[x] >= N || omega[x] >= N) return TD_ERR_ARG;
+            seen_b |= 1u << beta[x];
+            seen_o |= 1u << omega[x];
+        }
+        const uint32_t all = (N == 32) ? ~0u : ((1u << N) - 1u);
+        if (seen_b != all || seen_o != all) return TD_ERR_ARG;
+        uint8_t next_of[TD_MAX_N], rho[TD_MAX_N], sigma[TD_MAX_N];
+        for (int x = 0; x < N; ++x) next_of[beta[x]] = beta[(x + 1) % N];
+        for (int x = 0; x < N; ++x) rho[x] = omega[next_of[x]];
+        int r = beta[0];
+        for (int m = 0; m < N; ++m) { sigma[r] = (uint8_t)m; r = rho[r]; }
+        if (r != beta[0]) return TD_ERR_ARG;
+        for (int x = 0; x < N; ++x) {  // rho must visit every symbol once
+            int steps = 0, y = x;
+            do { y = rho[y]; ++steps; } while (y != x && steps <= N);
+            if (steps != N) return TD_ERR_ARG;
+        }
+        L = 0;
+        for (int m = 0; m < 16; ++m) {
+            const uint64_t v = (m < N - 1) ? (uint64_t)(sigma[beta[m + 1]] - 1) : (uint64_t)m;
+            L |= v << (4 * m);
+        }
+    }
+    out->perm = L;
+    out->min_rate = min_rate;
+    out->n_symbols = (uint8_t)N;
+    out->offset = 0;
+    out->max_moves = (uint8_t)max_moves;
+    out->packed = (uint8_t)((init & 31) | (full ? 0x80 : 0));
+    return 0;
+}
+
+// S_n permutation pi (values 0..n-1) -> the reference pair over N = n+1
+// symbols: beta = (0 1 ... n), rho = (0, pi0+1, ..., pi_{n-1}+1),
+// omega = rho . beta^-1, initialEvenCycles = odd cycles of omega.
+TD_HD void td_perm_to_pair(const int8_t *pi, int n, uint8_t *beta, uint8_t *omega, int *init) {
+    const int N = n + 1;
+    uint8_t seq[TD_MAX_N], rho[TD_MAX_N];
+    seq[0] = 0;
+    for (int m = 0; m < n; ++m) seq[m + 1] = (uint8_t)(pi[m] + 1);
+    for (int m = 0; m < N; ++m) rho[seq[m]] = seq[(m + 1) % N];
+    for (int x = 0; x < N; ++x) {
+        beta[x] = (uint8_t)x;
+        omega[x] = rho[(x + N - 1) % N];
+    }
+    *init = td_count_odd_cycles(omega, N);
+}

@@ -1,0 +1,750 @@
+// td_engine.cu -- kernels and host C ABI of the B200 witness-search engine.
+//
+// Kernels
+//   td_plain_kernel       one warp per instance, one launch per batch
+//   td_persistent_kernel  resident grid; warps claim instances with an atomic
+//                         ticket (steal granularity = instances per claim)
+//   td_validate_kernel    replays witnesses in pinned form
+// Host
+//   slots (stream + completion event + device scratch per slot) with the
+//   reference's initSlots / searchForSortingSeq semantics, batch entry points,
+//   instance preparation and the seeded synthetic generator.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "td_kernels.cuh"
+
+#define TD_API extern "C" __attribute__((visibility("default")))
+
+// mirrors include/td16_b200.h
+#define TD_OK 0
+#define TD_NOT_FOUND_RC 1
+#define TD_OVERFLOW 2
+#define TD_CUDA_ERROR 3
+#define TD_INVALID_ARG 4
+#define TD_TIMEOUT 5
+#define TD_FLAG_PLAIN 2u
+#define TD_FLAG_VERIFY 4u
+#define TD_ERR_VERIFY (-6)
+
+struct td_batch_stats {
+    uint64_t expansions, found, not_found, errors;
+    float kernel_ms;
+};
+
+static_assert(sizeof(td_instance) == 16, "td_instance layout");
+static_assert(sizeof(td_result) == 32, "td_result layout");
+
+// ============================================================================
+// kernels
+// ============================================================================
+
+#define TD_LUT_BYTES 4096
+
+__device__ __forceinline__ void td_block_init(uint8_t *lut, td_warp_smem *ws, int warps) {
+    for (int i = threadIdx.x; i < TD_LUT_BYTES; i += blockDim.x) lut[i] = (uint8_t)td_class_of_index(i);
+    for (int w = 0; w < warps; ++w)
+        for (int b = threadIdx.x; b < TD_PT_STRIDE; b += blockDim.x) ws[w].pt[TD_PT_DUMMY + b] = 0;
+    __syncthreads();
+}
+
+__device__ __forceinline__ td_search_limits td_make_limits(uint64_t max_exp, uint64_t time_limit_ns,
+                                                           const int *abort_flag) {
+    td_search_limits lim;
+    lim.max_expansions = max_exp ? max_exp : ~0ull;
+    lim.deadline_ns = time_limit_ns ? td_globaltimer() + time_limit_ns : 0;
+    lim.abort_flag = abort_flag;
+    return lim;
+}
+
+template <bool ORDERED>
+__global__ void __launch_bounds__(256) td_plain_kernel(const td_instance *__restrict__ in,
+                                                      td_result *__restrict__ out, int count,
+                                                      uint64_t max_exp, uint64_t time_limit_ns) {
+    extern __shared__ __align__(16) uint8_t td_smem[];
+    const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5;
+    uint8_t *lut = td_smem;
+    td_warp_smem *ws = reinterpret_cast<td_warp_smem *>(td_smem + TD_LUT_BYTES);
+    td_block_init(lut, ws, warps);
+    const int idx = blockIdx.x * warps + warp;
+    if (idx >= count) return;
+    const td_search_limits lim = td_make_limits(max_exp, time_limit_ns, nullptr);
+    uint32_t code[TD_MAX_STEPS];
+    int codeN = -1;
+    const td_instance x = in[idx];
+    td_warp_search<ORDERED>(x, &out[idx], ws[warp], lut, code, codeN, lim);
+}
+
+template <bool ORDERED>
+__global__ void __launch_bounds__(256) td_persistent_kernel(const td_instance *__restrict__ in,
+                                                           td_result *__restrict__ out, int count,
+                                                           int *ticket, int grain, uint64_t max_exp,
+                                                           uint64_t time_limit_ns) {
+    extern __shared__ __align__(16) uint8_t td_smem[];
+    const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint8_t *lut = td_smem;
+    td_warp_smem *ws = reinterpret_cast<td_warp_smem *>(td_smem + TD_LUT_BYTES);
+    td_block_init(lut, ws, warps);
+    uint32_t code[TD_MAX_STEPS];
+    int codeN = -1;
+    const td_search_limits lim = td_make_limits(max_exp, time_limit_ns, nullptr);
+    for (;;) {
+        int first = 0;
+        if (lane == 0) first = atomicAdd(ticket, grain);
+        first = __shfl_sync(TD_FULL, first, 0);
+        if (first >= count) break;
+        const int last = min(count, first + grain);
+        for (int idx = first; idx < last; ++idx) {
+            const td_instance x = in[idx];
+            td_warp_search<ORDERED>(x, &out[idx], ws[warp], lut, code, codeN, lim);
+        }
+    }
+}
+
+// Witness replay in pinned form: every move must be an in-range position
+// triple i<j<k, at most max_moves of them, and the final state must be the
+// identity (omega = id  <=>  beta = rho  <=>  L = 0,1,...,n-1).
+__global__ void td_validate_kernel(const td_instance *__restrict__ in, td_result *__restrict__ res,
+                                   uint8_t *__restrict__ ok, int count, int mark) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= count) return;
+    const td_instance x = in[idx];
+    const td_result r = res[idx];
+    const int N = x.n_symbols;
+    uint8_t good = r.status == TD_FOUND && r.depth >= 1 && r.depth <= x.max_moves && N >= 3 && N <= TD_MAX_N;
+    uint64_t L = x.perm;
+    int off = x.offset;
+    for (int d = 0; good && d < r.depth; ++d) {
+        const int m = r.moves[d];
+        const int i = m & 31, j = (m >> 5) & 31, k = (m >> 10) & 31;
+        if (!(i < j && j < k && k < N)) { good = 0; break; }
+        uint64_t nL;
+        int noff;
+        td_apply_move(L, off, N, i, j, k, &nL, &noff);
+        L = nL;
+        off = noff;
+    }
+    uint64_t ident = 0;
+    for (int m = 0; m < 16; ++m) ident |= (uint64_t)m << (4 * m);
+    good = good && L == ident;
+    if (ok) ok[idx] = good;
+    if (mark && r.status == TD_FOUND && !good) res[idx].status = TD_ERR_VERIFY;
+}
+
+// Integer issue peak: independent LOP3 chains (ALU pipe) at full occupancy.
+// Each thread runs `iters` iterations of 16 lop3 operations over 8 registers.
+__global__ void __launch_bounds__(256) td_int_peak_kernel(uint32_t *sink, int iters) {
+    uint32_t a[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) a[c] = threadIdx.x * 0x9E3779B9u + c * 0x85EBCA6Bu + blockIdx.x;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                asm volatile("lop3.b32 %0, %0, %1, %2, 0x96;" : "+r"(a[c]) : "r"(a[(c + 1) & 7]), "r"(a[(c + 3) & 7]));
+            }
+        }
+    }
+    uint32_t x = 0;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) x ^= a[c];
+    if (x == 0x12345678u) sink[blockIdx.x] = x;
+}
+
+// ============================================================================
+// host side
+// ============================================================================
+
+namespace {
+
+struct Slot {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr, t0 = nullptr, t1 = nullptr;
+    size_t budget = 0;
+    td_instance *d_inst = nullptr;
+    td_result *d_res = nullptr;
+    td_instance *h_inst = nullptr;
+    td_result *h_res = nullptr;
+    int *d_ticket = nullptr;
+    void *d_batch = nullptr;
+    size_t d_batch_bytes = 0;
+    std::mutex *mu = nullptr;
+};
+
+struct DeviceInfo {
+    bool ready = false;
+    int sms = 0;
+    int blocks_per_sm = 0;
+};
+
+std::mutex g_mu;
+std::vector<Slot> g_slots;
+std::vector<DeviceInfo> g_dev;
+
+int g_warps_per_block = 4;
+int g_grain = 1;
+
+void set_err(char *err, size_t len, const std::string &msg) {
+    if (err && len) {
+        std::snprintf(err, len, "%s", msg.c_str());
+    }
+}
+
+std::string cuda_msg(cudaError_t e, const char *file, int line) {
+    return std::string(file) + ":" + std::to_string(line) + ": CUDA error " + cudaGetErrorName(e) + " (" +
+           cudaGetErrorString(e) + ")";
+}
+
+#define TD_CHECK(call)                                                   \
+    do {                                                                 \
+        cudaError_t e_ = (call);                                         \
+        if (e_ != cudaSuccess) {                                         \
+            set_err(err, errlen, cuda_msg(e_, __FILE__, __LINE__));      \
+            return TD_CUDA_ERROR;                                        \
+        }                                                                \
+    } while (0)
+
+size_t smem_bytes(int warps) { return TD_LUT_BYTES + (size_t)warps * sizeof(td_warp_smem); }
+
+uint64_t time_limit_ns() {
+    static uint64_t v = [] {
+        const char *s = std::getenv("TD16_TIME_LIMIT_S");
+        double secs = s ? std::atof(s) : 300.0;
+        if (!(secs > 0)) secs = 300.0;
+        return (uint64_t)(secs * 1e9);
+    }();
+    return v;
+}
+
+int ensure_device(int device, char *err, size_t errlen) {
+    if ((int)g_dev.size() <= device) g_dev.resize(device + 1);
+    DeviceInfo &d = g_dev[device];
+    if (d.ready) return TD_OK;
+    TD_CHECK(cudaSetDevice(device));
+    std::vector<uint16_t> tri(TD_TRI_TABLE, 0);
+    for (int N = 3; N <= TD_MAX_N; ++N) {
+        int base = N < 4 ? 0 : N * (N - 1) * (N - 2) * (N - 3) / 24, t = 0;
+        for (int i = 0; i < N - 2; ++i)
+            for (int j = i + 1; j < N - 1; ++j)
+                for (int k = j + 1; k < N; ++k) tri[base + t++] = td_pack_move(i, j, k);
+    }
+    TD_CHECK(cudaMemcpyToSymbol(td_tri_table, tri.data(), tri.size() * sizeof(uint16_t)));
+    TD_CHECK(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device));
+    const int max_warps = 8;
+    const size_t max_smem = smem_bytes(max_warps);
+    TD_CHECK(cudaFuncSetAttribute(td_plain_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
+    TD_CHECK(cudaFuncSetAttribute(td_plain_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
+    TD_CHECK(cudaFuncSetAttribute(td_persistent_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
+    TD_CHECK(cudaFuncSetAttribute(td_persistent_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
+    d.ready = true;
+    return TD_OK;
+}
+
+void release_slot(Slot &s) {
+    if (s.device >= 0) cudaSetDevice(s.device);
+    if (s.stream) cudaStreamSynchronize(s.stream);
+    if (s.d_inst) cudaFree(s.d_inst);
+    if (s.d_res) cudaFree(s.d_res);
+    if (s.d_ticket) cudaFree(s.d_ticket);
+    if (s.d_batch) cudaFree(s.d_batch);
+    if (s.h_inst) cudaFreeHost(s.h_inst);
+    if (s.h_res) cudaFreeHost(s.h_res);
+    if (s.done) cudaEventDestroy(s.done);
+    if (s.t0) cudaEventDestroy(s.t0);
+    if (s.t1) cudaEventDestroy(s.t1);
+    if (s.stream) cudaStreamDestroy(s.stream);
+    delete s.mu;
+    s = Slot{};
+}
+
+void destroy_all() {
+    for (auto &s : g_slots) release_slot(s);
+    g_slots.clear();
+}
+
+// Launch one batch on `stream`.  Instances and results are device pointers.
+int launch_batch(Slot &s, int count, const td_instance *d_in, td_result *d_out, unsigned flags,
+                 uint64_t max_exp, cudaStream_t stream, char *err, size_t errlen) {
+    if (count <= 0) return TD_OK;
+    const bool ordered = flags & TD_FLAG_ORDERED;
+    const int warps = g_warps_per_block;
+    const size_t smem = smem_bytes(warps);
+    const int threads = warps * 32;
+    if (flags & TD_FLAG_PLAIN) {
+        const int blocks = (count + warps - 1) / warps;
+        if (ordered) td_plain_kernel<true><<<blocks, threads, smem, stream>>>(d_in, d_out, count, max_exp, time_limit_ns());
+        else td_plain_kernel<false><<<blocks, threads, smem, stream>>>(d_in, d_out, count, max_exp, time_limit_ns());
+    } else {
+        DeviceInfo &d = g_dev[s.device];
+        if (d.blocks_per_sm == 0) {
+            int b = 0;
+            TD_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, td_persistent_kernel<false>, threads, smem));
+            d.blocks_per_sm = std::max(1, b);
+        }
+        const int grid_max = d.sms * d.blocks_per_sm;
+        const int grid = std::max(1, std::min(grid_max, (count + warps - 1) / warps));
+        TD_CHECK(cudaMemsetAsync(s.d_ticket, 0, sizeof(int), stream));
+        if (ordered)
+            td_persistent_kernel<true><<<grid, threads, smem, stream>>>(d_in, d_out, count, s.d_ticket, g_grain, max_exp, time_limit_ns());
+        else
+            td_persistent_kernel<false><<<grid, threads, smem, stream>>>(d_in, d_out, count, s.d_ticket, g_grain, max_exp, time_limit_ns());
+    }
+    TD_CHECK(cudaGetLastError());
+    if (flags & TD_FLAG_VERIFY) {
+        td_validate_kernel<<<(count + 255) / 256, 256, 0, stream>>>(d_in, d_out, nullptr, count, 1);
+        TD_CHECK(cudaGetLastError());
+    }
+    return TD_OK;
+}
+
+Slot *get_slot(int slot, char *err, size_t errlen) {
+    if (slot < 0 || slot >= (int)g_slots.size() || g_slots[slot].device < 0) {
+        set_err(err, errlen, "invalid GPU sorting slot");
+        return nullptr;
+    }
+    return &g_slots[slot];
+}
+
+int search_one(int slot, const uint8_t *beta, const uint8_t *omega, int n, int init, float min_rate,
+               int max_moves, int full, int16_t *out_ijk, int *out_depth, unsigned flags, char *err,
+               size_t errlen) {
+    if (out_depth) *out_depth = 0;
+    if (!beta || !omega) {
+        set_err(err, errlen, "beta and omega must not be null");
+        return TD_INVALID_ARG;
+    }
+    if (n > TD_MAX_N) {
+        set_err(err, errlen, "performGpuSortingSearch: n exceeds MAX_N");
+        return TD_INVALID_ARG;
+    }
+    if (max_moves <= 0 || max_moves > TD_MAX_DEPTH) {
+        set_err(err, errlen, "performGpuSortingSearch: invalid maximumDepth");
+        return TD_INVALID_ARG;
+    }
+    Slot *s;
+    {
+        std::lock_guard<std::mutex> g(g_mu);
+        s = get_slot(slot, err, errlen);
+        if (!s) return TD_INVALID_ARG;
+    }
+    if (td_triple_count(n) == 0) return TD_NOT_FOUND_RC;
+    td_instance x;
+    if (td_prepare_pair(beta, omega, n, init, min_rate, max_moves, full, &x) != 0) {
+        set_err(err, errlen, "beta/omega are not permutations whose product omega.beta is an n-cycle");
+        return TD_INVALID_ARG;
+    }
+    std::lock_guard<std::mutex> g(*s->mu);
+    TD_CHECK(cudaSetDevice(s->device));
+    *s->h_inst = x;
+    TD_CHECK(cudaMemcpyAsync(s->d_inst, s->h_inst, sizeof(td_instance), cudaMemcpyHostToDevice, s->stream));
+    int rc = launch_batch(*s, 1, s->d_inst, s->d_res, flags | TD_FLAG_PLAIN, 0, s->stream, err, errlen);
+    if (rc != TD_OK) return rc;
+    TD_CHECK(cudaMemcpyAsync(s->h_res, s->d_res, sizeof(td_result), cudaMemcpyDeviceToHost, s->stream));
+    TD_CHECK(cudaEventRecord(s->done, s->stream));
+    TD_CHECK(cudaEventSynchronize(s->done));
+    const td_result r = *s->h_res;
+    if (r.status == TD_FOUND) {
+        for (int d = 0; d < r.depth; ++d) {
+            out_ijk[3 * d + 0] = (int16_t)(r.moves[d] & 31);
+            out_ijk[3 * d + 1] = (int16_t)((r.moves[d] >> 5) & 31);
+            out_ijk[3 * d + 2] = (int16_t)((r.moves[d] >> 10) & 31);
+        }
+        if (out_depth) *out_depth = r.depth;
+        return TD_OK;
+    }
+    if (r.status == TD_NOT_FOUND) return TD_NOT_FOUND_RC;
+    if (r.status == TD_ERR_BUDGET) {
+        set_err(err, errlen, "GPU sorting search queue overflow");
+        return TD_OVERFLOW;
+    }
+    if (r.status == TD_ERR_TIMEOUT) {
+        set_err(err, errlen, "GPU sorting search deadline reached");
+        return TD_TIMEOUT;
+    }
+    set_err(err, errlen, "GPU sorting search rejected its input");
+    return TD_INVALID_ARG;
+}
+
+// ---- seeded synthetic instances ----------------------------------------------
+
+inline uint64_t splitmix64(uint64_t &s) {
+    uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// Lemire's multiply-shift bounded draw on the upper 32 bits, with rejection.
+inline uint32_t bounded(uint64_t &s, uint32_t range) {
+    uint32_t x = (uint32_t)(splitmix64(s) >> 32);
+    uint64_t m = (uint64_t)x * range;
+    uint32_t l = (uint32_t)m;
+    if (l < range) {
+        const uint32_t t = (0u - range) % range;
+        while (l < t) {
+            x = (uint32_t)(splitmix64(s) >> 32);
+            m = (uint64_t)x * range;
+            l = (uint32_t)m;
+        }
+    }
+    return (uint32_t)(m >> 32);
+}
+
+// lexicographic unranking of r over triples x<y<z of {0..n}
+void unrank_triple(int n, uint32_t r, int *x, int *y, int *z) {
+    const int M = n + 1;
+    for (int a = 0; a < M - 2; ++a) {
+        const uint32_t c = (uint32_t)((M - a - 1) * (M - a - 2) / 2);
+        if (r < c) {
+            for (int b = a + 1; b < M - 1; ++b) {
+                const uint32_t cb = (uint32_t)(M - b - 1);
+                if (r < cb) {
+                    *x = a;
+                    *y = b;
+                    *z = b + 1 + (int)r;
+                    return;
+                }
+                r -= cb;
+            }
+        }
+        r -= c;
+    }
+    *x = 0;
+    *y = 1;
+    *z = 2;
+}
+
+}  // namespace
+
+// ============================================================================
+// C ABI
+// ============================================================================
+
+TD_API int td_init_slots(int total_slots, const int *devices, int device_count, uint64_t budget, char *err,
+                         size_t errlen) {
+    if (!devices || device_count <= 0) {
+        set_err(err, errlen, "devices must contain at least one CUDA device ordinal");
+        return TD_INVALID_ARG;
+    }
+    if (total_slots <= 0) {
+        set_err(err, errlen, "totalSlots must be positive");
+        return TD_INVALID_ARG;
+    }
+    if (budget == 0) {
+        set_err(err, errlen, "queueBytesBudget must be positive");
+        return TD_INVALID_ARG;
+    }
+    int ndev = 0;
+    TD_CHECK(cudaGetDeviceCount(&ndev));
+    std::vector<int> per(ndev > 0 ? ndev : 1, 0);
+    for (int i = 0; i < device_count; ++i) {
+        if (devices[i] < 0 || devices[i] >= ndev) {
+            set_err(err, errlen, "devices contains a CUDA device ordinal outside the available range");
+            return TD_INVALID_ARG;
+        }
+        for (int j = 0; j < i; ++j)
+            if (devices[j] == devices[i]) {
+                set_err(err, errlen, "devices must contain distinct CUDA device ordinals");
+                return TD_INVALID_ARG;
+            }
+    }
+    for (int i = 0; i < total_slots; ++i) per[devices[i % device_count]]++;
+    std::lock_guard<std::mutex> g(g_mu);
+    destroy_all();
+    for (int i = 0; i < device_count; ++i) {
+        const int dev = devices[i];
+        TD_CHECK(cudaSetDevice(dev));
+        size_t free_b = 0, total_b = 0;
+        TD_CHECK(cudaMemGetInfo(&free_b, &total_b));
+        const uint64_t need = budget * (uint64_t)per[dev];
+        if (per[dev] > 0 && (budget > UINT64_MAX / (uint64_t)per[dev] || need > free_b)) {
+            set_err(err, errlen, "CUDA device " + std::to_string(dev) + " has " + std::to_string(free_b) +
+                                     " free bytes, but its search queues require at least " +
+                                     std::to_string(need) + " bytes");
+            return TD_INVALID_ARG;
+        }
+        int rc = ensure_device(dev, err, errlen);
+        if (rc != TD_OK) return rc;
+    }
+    g_slots.resize(total_slots);
+    for (int i = 0; i < total_slots; ++i) {
+        Slot &s = g_slots[i];
+        s.device = devices[i % device_count];
+        s.budget = budget;
+        s.mu = new std::mutex();
+        cudaError_t e = cudaSetDevice(s.device);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.done, cudaEventBlockingSync | cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreate(&s.t0);
+        if (e == cudaSuccess) e = cudaEventCreate(&s.t1);
+        if (e == cudaSuccess) e = cudaMalloc(&s.d_inst, sizeof(td_instance));
+        if (e == cudaSuccess) e = cudaMalloc(&s.d_res, sizeof(td_result));
+        if (e == cudaSuccess) e = cudaMalloc(&s.d_ticket, sizeof(int));
+        if (e == cudaSuccess) e = cudaMallocHost(&s.h_inst, sizeof(td_instance));
+        if (e == cudaSuccess) e = cudaMallocHost(&s.h_res, sizeof(td_result));
+        if (e != cudaSuccess) {
+            set_err(err, errlen, cuda_msg(e, __FILE__, __LINE__));
+            destroy_all();
+            return TD_CUDA_ERROR;
+        }
+    }
+    return TD_OK;
+}
+
+TD_API int td_search(int slot, const uint8_t *beta, const uint8_t *omega, int n, int init, float min_rate,
+                     int max_moves, int full, int16_t *out_ijk, int *out_depth, char *err, size_t errlen) {
+    return search_one(slot, beta, omega, n, init, min_rate, max_moves, full, out_ijk, out_depth, 0u, err, errlen);
+}
+
+TD_API int td_search_ordered(int slot, const uint8_t *beta, const uint8_t *omega, int n, int init,
+                             float min_rate, int max_moves, int full, int16_t *out_ijk, int *out_depth,
+                             char *err, size_t errlen) {
+    return search_one(slot, beta, omega, n, init, min_rate, max_moves, full, out_ijk, out_depth,
+                      TD_FLAG_ORDERED, err, errlen);
+}
+
+TD_API int td_slot_count(void) {
+    std::lock_guard<std::mutex> g(g_mu);
+    return (int)g_slots.size();
+}
+
+TD_API int td_slot_device(int slot) {
+    std::lock_guard<std::mutex> g(g_mu);
+    if (slot < 0 || slot >= (int)g_slots.size()) return -1;
+    return g_slots[slot].device;
+}
+
+TD_API void *td_slot_stream(int slot) {
+    std::lock_guard<std::mutex> g(g_mu);
+    if (slot < 0 || slot >= (int)g_slots.size()) return nullptr;
+    return (void *)g_slots[slot].stream;
+}
+
+TD_API int td_destroy(void) {
+    std::lock_guard<std::mutex> g(g_mu);
+    destroy_all();
+    return TD_OK;
+}
+
+TD_API int td_configure(int warps_per_block, int grain) {
+    if (warps_per_block < 1 || warps_per_block > 8 || grain < 1) return TD_INVALID_ARG;
+    std::lock_guard<std::mutex> g(g_mu);
+    g_warps_per_block = warps_per_block;
+    g_grain = grain;
+    for (auto &d : g_dev) d.blocks_per_sm = 0;
+    return TD_OK;
+}
+
+TD_API int td_prepare_pairs(int count, const uint8_t *beta, const uint8_t *omega, const uint8_t *n,
+                            const int32_t *init, const float *min_rate, const int32_t *max_moves,
+                            const uint8_t *full, td_instance *out, int *bad) {
+    for (int i = 0; i < count; ++i) {
+        if (td_prepare_pair(beta + (size_t)i * TD_MAX_N, omega + (size_t)i * TD_MAX_N, n[i], init[i], min_rate[i],
+                            max_moves[i], full[i], &out[i]) != 0) {
+            if (bad) *bad = i;
+            return TD_INVALID_ARG;
+        }
+    }
+    return TD_OK;
+}
+
+TD_API int td_prepare_perms(int count, const int8_t *perms, const uint8_t *n, const int32_t *max_moves,
+                            float min_rate, int full, td_instance *out, int *bad) {
+    for (int i = 0; i < count; ++i) {
+        const int ni = n[i];
+        uint8_t beta[TD_MAX_N], omega[TD_MAX_N];
+        int init = 0;
+        bool okp = ni >= 0 && ni < TD_MAX_N;
+        if (okp) {
+            uint32_t seen = 0;
+            for (int m = 0; m < ni; ++m) {
+                const int v = perms[(size_t)i * 16 + m];
+                if (v < 0 || v >= ni || (seen >> v) & 1u) okp = false;
+                else seen |= 1u << v;
+            }
+        }
+        if (okp) {
+            td_perm_to_pair(perms + (size_t)i * 16, ni, beta, omega, &init);
+            okp = td_prepare_pair(beta, omega, ni + 1, init, min_rate, max_moves[i], full, &out[i]) == 0;
+        }
+        if (!okp) {
+            if (bad) *bad = i;
+            return TD_INVALID_ARG;
+        }
+    }
+    return TD_OK;
+}
+
+TD_API int td_synth_perms(uint64_t seed, int count, int n_min, int n_max, int hard_pct, int hard_min, int hard_max,
+                          int8_t *perms, uint8_t *n_out) {
+    if (n_min < 1 || n_max > 16 || n_min > n_max || hard_min < 0 || hard_max < hard_min) return TD_INVALID_ARG;
+    for (int i = 0; i < count; ++i) {
+        uint64_t st = seed ^ (uint64_t)i;
+        const int n = n_min + (int)bounded(st, (uint32_t)(n_max - n_min + 1));
+        int8_t *p = perms + (size_t)i * 16;
+        const bool hard = (int)bounded(st, 100) < hard_pct;
+        if (hard) {
+            for (int m = 0; m < n; ++m) p[m] = (int8_t)(n - 1 - m);
+            const int moves = hard_min + (int)bounded(st, (uint32_t)(hard_max - hard_min + 1));
+            const uint32_t triples = (uint32_t)((n + 1) * n * (n - 1) / 6);
+            for (int mv = 0; mv < moves && triples > 0; ++mv) {
+                int x, y, z;
+                unrank_triple(n, bounded(st, triples), &x, &y, &z);
+                int8_t tmp[16];
+                int w = 0;
+                for (int q = 0; q < x; ++q) tmp[w++] = p[q];
+                for (int q = y; q < z; ++q) tmp[w++] = p[q];
+                for (int q = x; q < y; ++q) tmp[w++] = p[q];
+                for (int q = z; q < n; ++q) tmp[w++] = p[q];
+                std::memcpy(p, tmp, (size_t)n);
+            }
+        } else {
+            for (int m = 0; m < n; ++m) p[m] = (int8_t)m;
+            for (int m = n - 1; m > 0; --m) {
+                const int j = (int)bounded(st, (uint32_t)(m + 1));
+                const int8_t t = p[m];
+                p[m] = p[j];
+                p[j] = t;
+            }
+        }
+        for (int m = n; m < 16; ++m) p[m] = 0;
+        n_out[i] = (uint8_t)n;
+    }
+    return TD_OK;
+}
+
+TD_API int td_search_batch_device(int slot, int count, const td_instance *d_in, td_result *d_out, unsigned flags,
+                                  uint64_t max_exp, void *stream, char *err, size_t errlen) {
+    Slot *s;
+    {
+        std::lock_guard<std::mutex> g(g_mu);
+        s = get_slot(slot, err, errlen);
+        if (!s) return TD_INVALID_ARG;
+    }
+    if (count < 0 || (count > 0 && (!d_in || !d_out))) {
+        set_err(err, errlen, "invalid batch arguments");
+        return TD_INVALID_ARG;
+    }
+    std::lock_guard<std::mutex> g(*s->mu);
+    TD_CHECK(cudaSetDevice(s->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+    return launch_batch(*s, count, d_in, d_out, flags, max_exp, st, err, errlen);
+}
+
+TD_API int td_search_batch(int slot, int count, const td_instance *in, td_result *out, unsigned flags,
+                           uint64_t max_exp, td_batch_stats *stats, char *err, size_t errlen) {
+    Slot *s;
+    {
+        std::lock_guard<std::mutex> g(g_mu);
+        s = get_slot(slot, err, errlen);
+        if (!s) return TD_INVALID_ARG;
+    }
+    if (count < 0 || (count > 0 && (!in || !out))) {
+        set_err(err, errlen, "invalid batch arguments");
+        return TD_INVALID_ARG;
+    }
+    std::lock_guard<std::mutex> g(*s->mu);
+    TD_CHECK(cudaSetDevice(s->device));
+    const size_t need = (size_t)count * (sizeof(td_instance) + sizeof(td_result));
+    if (need > s->d_batch_bytes) {
+        if (s->d_batch) TD_CHECK(cudaFree(s->d_batch));
+        s->d_batch = nullptr;
+        s->d_batch_bytes = 0;
+        TD_CHECK(cudaMalloc(&s->d_batch, need));
+        s->d_batch_bytes = need;
+    }
+    td_instance *d_in = (td_instance *)s->d_batch;
+    td_result *d_out = (td_result *)((char *)s->d_batch + (size_t)count * sizeof(td_instance));
+    TD_CHECK(cudaMemcpyAsync(d_in, in, (size_t)count * sizeof(td_instance), cudaMemcpyHostToDevice, s->stream));
+    TD_CHECK(cudaEventRecord(s->t0, s->stream));
+    int rc = launch_batch(*s, count, d_in, d_out, flags, max_exp, s->stream, err, errlen);
+    if (rc != TD_OK) return rc;
+    TD_CHECK(cudaEventRecord(s->t1, s->stream));
+    TD_CHECK(cudaMemcpyAsync(out, d_out, (size_t)count * sizeof(td_result), cudaMemcpyDeviceToHost, s->stream));
+    TD_CHECK(cudaEventRecord(s->done, s->stream));
+    TD_CHECK(cudaEventSynchronize(s->done));
+    if (stats) {
+        std::memset(stats, 0, sizeof *stats);
+        TD_CHECK(cudaEventElapsedTime(&stats->kernel_ms, s->t0, s->t1));
+        for (int i = 0; i < count; ++i) {
+            stats->expansions += out[i].expansions;
+            if (out[i].status == TD_FOUND) stats->found++;
+            else if (out[i].status == TD_NOT_FOUND) stats->not_found++;
+            else stats->errors++;
+        }
+    }
+    return TD_OK;
+}
+
+TD_API int td_validate_batch_device(int count, const td_instance *d_in, const td_result *d_res, uint8_t *d_ok,
+                                    void *stream, char *err, size_t errlen) {
+    if (count <= 0) return TD_OK;
+    const int threads = 256;
+    td_validate_kernel<<<(count + threads - 1) / threads, threads, 0, (cudaStream_t)stream>>>(
+        d_in, const_cast<td_result *>(d_res), d_ok, count, 0);
+    TD_CHECK(cudaGetLastError());
+    return TD_OK;
+}
+
+TD_API void td_positions_to_symbols(const uint8_t *beta, int n, const int16_t *ijk, int depth, uint8_t *out_abc) {
+    uint8_t cur[TD_MAX_N], nxt[TD_MAX_N];
+    std::memcpy(cur, beta, (size_t)n);
+    for (int d = 0; d < depth; ++d) {
+        const int i = ijk[3 * d], j = ijk[3 * d + 1], k = ijk[3 * d + 2];
+        out_abc[3 * d] = cur[i];
+        out_abc[3 * d + 1] = cur[j];
+        out_abc[3 * d + 2] = cur[k];
+        int w = 0;
+        for (int q = 0; q < i; ++q) nxt[w++] = cur[q];
+        for (int q = j; q < k; ++q) nxt[w++] = cur[q];
+        for (int q = i; q < j; ++q) nxt[w++] = cur[q];
+        for (int q = k; q < n; ++q) nxt[w++] = cur[q];
+        std::memcpy(cur, nxt, (size_t)n);
+    }
+}
+
+// Measures the ALU-pipe integer issue rate of `device` in warp instructions
+// per second (LOP3 only), at full occupancy, over about `target_ms`.
+TD_API int td_int_issue_peak(int device, float target_ms, double *warp_inst_per_s, double *ms_out, char *err,
+                             size_t errlen) {
+    TD_CHECK(cudaSetDevice(device));
+    int sms = 0;
+    TD_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    int per_sm = 0;
+    TD_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, td_int_peak_kernel, 256, 0));
+    const int blocks = sms * std::max(1, per_sm);
+    uint32_t *sink = nullptr;
+    TD_CHECK(cudaMalloc(&sink, sizeof(uint32_t) * blocks));
+    cudaEvent_t a, b;
+    TD_CHECK(cudaEventCreate(&a));
+    TD_CHECK(cudaEventCreate(&b));
+    int iters = 1024;
+    float ms = 0;
+    for (int attempt = 0; attempt < 12; ++attempt) {
+        td_int_peak_kernel<<<blocks, 256>>>(sink, iters);  // warm-up at this size
+        TD_CHECK(cudaEventRecord(a));
+        td_int_peak_kernel<<<blocks, 256>>>(sink, iters);
+        TD_CHECK(cudaEventRecord(b));
+        TD_CHECK(cudaEventSynchronize(b));
+        TD_CHECK(cudaEventElapsedTime(&ms, a, b));
+        if (ms >= target_ms) break;
+        iters *= 2;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(sink);
+    const double warp_insts = (double)blocks * (256 / 32) * (double)iters * 16.0;
+    if (warp_inst_per_s) *warp_inst_per_s = warp_insts / (ms * 1e-3);
+    if (ms_out) *ms_out = ms;
+    return TD_OK;
+}

@@ -1,0 +1,350 @@
+// td_kernels.cuh -- the sm_100a witness-search warp engine.
+//
+// One warp owns one search (a DFS over move sequences).  Per node it
+//   1. labels the omega cycles of the pinned state with warp pointer jumping
+//      (lane p = pinned position p; leader = smallest position, dist = steps
+//      to the leader, len = cycle length; 5 rounds cover cycles up to 32),
+//   2. writes the pair table (4 bits per ordered pair of caller positions),
+//   3. evaluates every triple: lane l takes u = 32*s + l in step s, reads three
+//      pair entries and one class-table byte (no pointer chasing), and keeps
+//      one bit per step in per-lane masks (found / first-choice / second-choice),
+//   4. picks the next child with a warp max-reduction over the masks in the
+//      reference's single-queue order (ordered mode) or +2 moves first.
+// Reference: emitter/src/native/backtracking/sorting_search.cu:478-712.
+#pragma once
+
+#include "td_core.cuh"
+
+#define TD_FULL 0xffffffffu
+#define TD_PT_ROWS 18          // 17 position rows + one zero row for idle lanes
+#define TD_PT_DUMMY (17 * TD_PT_STRIDE)
+#define TD_TRI_TABLE 3060      // sum over N <= 17 of C(N,3) = C(18,4)
+
+// Per-warp shared state.
+struct td_warp_smem {
+    uint8_t pt[TD_PT_ROWS * TD_PT_STRIDE];     // pair table of the current node
+    uint32_t m1[TD_MAX_DEPTH][32];             // per level, per lane step masks
+    uint32_t m2[TD_MAX_DEPTH][32];
+    uint64_t L[TD_MAX_DEPTH + 1];              // pinned state per level
+    uint32_t acc[TD_MAX_DEPTH + 2];            // accept mask over odd counts, per depth
+    uint32_t reach[TD_MAX_DEPTH + 2];          // prune mask over odd counts, per depth
+    uint16_t path[TD_MAX_DEPTH];               // caller-position move per level
+    uint8_t off[TD_MAX_DEPTH + 1];
+};
+
+// Lexicographic position triples i|j<<5|k<<10 for every N, at offset C(N,4).
+__device__ uint16_t td_tri_table[TD_TRI_TABLE];
+
+__device__ __forceinline__ int td_tri_base(int N) {
+    return N < 4 ? 0 : N * (N - 1) * (N - 2) * (N - 3) / 24;
+}
+
+// Load this lane's per-step pair-table offsets for triples of size N.
+__device__ __forceinline__ void td_load_codes(int N, uint32_t (&code)[TD_MAX_STEPS]) {
+    const int lane = threadIdx.x & 31;
+    const int T = td_triple_count(N);
+    const int base = td_tri_base(N);
+#pragma unroll
+    for (int s = 0; s < TD_MAX_STEPS; ++s) {
+        const int u = 32 * s + lane;
+        uint32_t c = TD_PT_DUMMY | (TD_PT_DUMMY << 10) | (TD_PT_DUMMY << 20);
+        if (u < T) {
+            const uint32_t t = td_tri_table[base + T - 1 - u];
+            const uint32_t i = t & 31, j = (t >> 5) & 31, k = (t >> 10) & 31;
+            c = (i * TD_PT_STRIDE + j) | ((j * TD_PT_STRIDE + k) << 10) | ((k * TD_PT_STRIDE + i) << 20);
+        }
+        code[s] = c;
+    }
+}
+
+// Cycle labels and pair table for the state (L, off); returns the number of
+// odd-length omega cycles.
+__device__ __forceinline__ int td_prepare_node(td_warp_smem &s, uint64_t L, int off, int N) {
+    const int p = threadIdx.x & 31;
+    const bool act = p < N;
+    const uint32_t Bp = p == 0 ? 0u : td_nib(L, p - 1) + 1u;
+    // inverse of L by a warp OR of one nibble per lane
+    uint32_t lo = 0, hi = 0;
+    if (p < N - 1) {
+        const uint64_t c = (uint64_t)p << (4 * td_nib(L, p));
+        lo = (uint32_t)c;
+        hi = (uint32_t)(c >> 32);
+    }
+    lo = __reduce_or_sync(TD_FULL, lo);
+    hi = __reduce_or_sync(TD_FULL, hi);
+    const uint64_t inv = ((uint64_t)hi << 32) | lo;
+    // omega(B[p]) = B[p-1] + 1 (mod N): next position along omega
+    const uint32_t Bq = __shfl_sync(TD_FULL, Bp, p == 0 ? N - 1 : p - 1);
+    uint32_t y = Bq + 1;
+    if (y == (uint32_t)N) y = 0;
+    const int nx = act ? (y ? (int)td_nib(inv, (int)y - 1) + 1 : 0) : p;
+    // leader = smallest position on the cycle
+    int m = p, j = nx;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+        const int mm = __shfl_sync(TD_FULL, m, j);
+        m = min(m, mm);
+        j = __shfl_sync(TD_FULL, j, j);
+    }
+    const bool leader = m == p;
+    // dist = omega steps to the leader (list ranking with the cycle cut there)
+    int d = leader ? 0 : 1;
+    j = leader ? p : nx;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+        d += __shfl_sync(TD_FULL, d, j);
+        j = __shfl_sync(TD_FULL, j, j);
+    }
+    const int after_leader = __shfl_sync(TD_FULL, nx, m);
+    const int len = __shfl_sync(TD_FULL, d, after_leader) + 1;
+    const int odd = __popc(__ballot_sync(TD_FULL, act && leader && (len & 1)));
+    // pair table row of this lane's caller position
+    const uint32_t md = (uint32_t)m | ((uint32_t)d << 8);
+    const uint32_t o3 = (uint32_t)(len & 1) << 3;
+    const uint32_t fixed4 = len == 1 ? 4u : 0u;
+    int rp = p - off;
+    rp += rp < 0 ? N : 0;
+    uint8_t *row = &s.pt[rp * TD_PT_STRIDE];
+    int q = off;  // pinned position of caller position 0
+    uint32_t word = 0;
+    for (int rq = 0; rq < N; ++rq) {
+        const uint32_t mdq = __shfl_sync(TD_FULL, md, q);
+        const uint32_t x = md ^ mdq;
+        uint32_t e;
+        if ((x & 0xffu) == 0) {
+            const uint32_t g = md > mdq ? 1u : 0u;  // same leader: compares dist
+            uint32_t w = (x >> 8) & 1u;              // parity of dist difference
+            w ^= (o3 >> 3) & (g ^ 1u);               // wrap of an odd cycle flips it
+            e = 1u | (w << 1) | (g << 2) | o3;
+        } else {
+            e = fixed4 | o3;
+        }
+        word |= e << (8 * (rq & 3));
+        if ((rq & 3) == 3 || rq == N - 1) {
+            if (act) *reinterpret_cast<uint32_t *>(row + (rq & ~3)) = word;
+            word = 0;
+        }
+        ++q;
+        q -= q >= N ? N : 0;
+    }
+    return odd;
+}
+
+// Accept / prune masks of one instance (lane o evaluates odd count o).
+__device__ __forceinline__ void td_rate_masks(td_warp_smem &s, const td_instance &x) {
+    const int o = threadIdx.x & 31;
+    const int N = x.n_symbols, init = td_inst_init(x), full = td_inst_full(x);
+    const int maxd = x.max_moves;
+#pragma unroll 1
+    for (int D = 0; D <= TD_MAX_DEPTH + 1; ++D) {
+        const unsigned a = __ballot_sync(TD_FULL, td_accepts(N, init, x.min_rate, full, o, D));
+        const unsigned r = __ballot_sync(TD_FULL, D < maxd && td_can_reach(N, init, x.min_rate, maxd, full, o, D));
+        if (o == 0) {
+            s.acc[D] = a;
+            s.reach[D] = r;
+        }
+    }
+    __syncwarp();
+}
+
+struct td_search_limits {
+    uint64_t max_expansions;   // per search; TD_ERR_BUDGET when exceeded
+    uint64_t deadline_ns;      // %globaltimer value; 0 = none
+    const int *abort_flag;     // optional host/device abort request
+};
+
+__device__ __forceinline__ uint64_t td_globaltimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Evaluate all children of the node at `level`.  Fills the level's masks and
+// returns the found child's u, or -1.
+template <bool ORDERED>
+__device__ __forceinline__ int td_evaluate(td_warp_smem &s, const uint8_t *lut,
+                                           const uint32_t (&code)[TD_MAX_STEPS], int steps,
+                                           int level, int odd, int maxd) {
+    const int lane = threadIdx.x & 31;
+    const int D = level + 1;
+    const uint32_t accD = s.acc[D], reachD = s.reach[D];
+    const uint32_t f0 = (accD >> odd) & 1u, f2 = (accD >> (odd + 2)) & 1u;
+    const uint32_t x0 = ((reachD >> odd) & 1u) & (f0 ^ 1u);
+    const uint32_t x2 = ((reachD >> (odd + 2)) & 1u) & (f2 ^ 1u);
+    const uint32_t nt = ORDERED
+        ? (((f0 | (x0 << 1)) << TD_CLASS_ZERO) | ((f2 | (x2 << 1)) << TD_CLASS_PLUS2))
+        : (((f0 | (x0 << 2)) << TD_CLASS_ZERO) | ((f2 | (x2 << 1)) << TD_CLASS_PLUS2));
+    (void)maxd;
+    __syncwarp();
+    uint32_t fb = 0, w1 = 0, w2 = 0;
+#pragma unroll
+    for (int st = 0; st < TD_MAX_STEPS; ++st) {
+        if (st < steps) {
+            const uint32_t c = code[st];
+            const uint32_t A = s.pt[c & 1023u];
+            const uint32_t B = s.pt[(c >> 10) & 1023u];
+            const uint32_t C = s.pt[c >> 20];
+            const uint32_t cls = lut[A | (B << 4) | (C << 8)];
+            const uint32_t tb = nt >> cls;
+            fb |= (tb & 1u) << st;
+            w1 |= ((tb >> 1) & 1u) << st;
+            if (!ORDERED) w2 |= ((tb >> 2) & 1u) << st;
+        }
+    }
+    if (ORDERED && level == 0) {  // roots are accepted on visit, not on seeding
+        s.m1[0][lane] = w1;
+        s.m2[0][lane] = fb;
+        return -1;
+    }
+    s.m1[level][lane] = w1;
+    if (!ORDERED) s.m2[level][lane] = w2;
+    if (__any_sync(TD_FULL, fb != 0)) {
+        const uint32_t key = fb ? ((uint32_t)(__ffs(fb) - 1) << 5) | (uint32_t)lane : 0xffffffffu;
+        return (int)__reduce_min_sync(TD_FULL, key);
+    }
+    return -1;
+}
+
+// Next child of `level`; returns u or -1.  *accepted is set for a root that
+// is accepted when visited (ordered mode).
+template <bool ORDERED>
+__device__ __forceinline__ int td_next_child(td_warp_smem &s, int level, int *accepted) {
+    const int lane = threadIdx.x & 31;
+    uint32_t a1 = s.m1[level][lane];
+    uint32_t a2 = ORDERED ? (level == 0 ? s.m2[0][lane] : 0u) : s.m2[level][lane];
+    const bool desc_lanes = ORDERED && level > 0;
+    uint32_t w;
+    bool use1 = true;
+    if (ORDERED) {
+        w = a1 | a2;
+    } else {
+        use1 = __any_sync(TD_FULL, a1 != 0);
+        w = use1 ? a1 : a2;
+    }
+    uint32_t key = 0;
+    if (w) key = ((31u - __clz(w)) << 5) + (uint32_t)(desc_lanes ? 31 - lane : lane) + 1u;
+    key = __reduce_max_sync(TD_FULL, key);
+    *accepted = 0;
+    if (key == 0) return -1;
+    key -= 1;
+    const int st = (int)(key >> 5);
+    const int win = desc_lanes ? 31 - (int)(key & 31) : (int)(key & 31);
+    const uint32_t bit = 1u << st;
+    if (ORDERED && level == 0) *accepted = __shfl_sync(TD_FULL, (a2 & bit) ? 1 : 0, win);
+    if (lane == win) {
+        if (ORDERED) {
+            s.m1[level][lane] = a1 & ~bit;
+            if (level == 0) s.m2[0][lane] = a2 & ~bit;
+        } else if (use1) {
+            s.m1[level][lane] = a1 & ~bit;
+        } else {
+            s.m2[level][lane] = a2 & ~bit;
+        }
+    }
+    __syncwarp();
+    return st * 32 + win;
+}
+
+// One complete search by the calling warp.  `code`/`codeN` cache the lane's
+// triple offsets for the last N seen.  Writes *out from lane 0.
+template <bool ORDERED>
+__device__ void td_warp_search(const td_instance &x, td_result *out, td_warp_smem &s,
+                               const uint8_t *lut, uint32_t (&code)[TD_MAX_STEPS], int &codeN,
+                               const td_search_limits &lim) {
+    const int lane = threadIdx.x & 31;
+    const int N = x.n_symbols;
+    const int maxd = x.max_moves;
+    const int T = td_triple_count(N);
+    int status = TD_NOT_FOUND, depth = 0;
+    uint32_t expansions = 0;
+    uint16_t found_move = 0;
+    if (N > TD_MAX_N || maxd < 1 || maxd > TD_MAX_DEPTH || td_inst_init(x) > TD_MAX_N) {
+        status = TD_ERR_ARG;
+    } else if (T > 0) {
+        if (codeN != N) {
+            td_load_codes(N, code);
+            codeN = N;
+        }
+        const int steps = (T + 31) >> 5;
+        const int tri_base = td_tri_base(N);
+        td_rate_masks(s, x);
+        if (lane == 0) {
+            s.L[0] = x.perm;
+            s.off[0] = x.offset;
+        }
+        __syncwarp();
+        int level = 0;
+        int odd = td_prepare_node(s, x.perm, x.offset, N);
+        int found = td_evaluate<ORDERED>(s, lut, code, steps, 0, odd, maxd);
+        expansions = 1;
+        for (;;) {
+            if (found >= 0) {
+                const uint32_t t = td_tri_table[tri_base + T - 1 - found];
+                found_move = (uint16_t)t;
+                depth = level + 1;
+                status = TD_FOUND;
+                break;
+            }
+            int accepted;
+            const int u = td_next_child<ORDERED>(s, level, &accepted);
+            if (u < 0) {
+                if (level == 0) break;  // exhausted: not found
+                --level;
+                continue;
+            }
+            const uint32_t t = td_tri_table[tri_base + T - 1 - u];
+            if (accepted) {
+                found_move = (uint16_t)t;
+                depth = level + 1;
+                status = TD_FOUND;
+                break;
+            }
+            if (expansions >= lim.max_expansions) {
+                status = TD_ERR_BUDGET;
+                break;
+            }
+            if ((expansions & 255u) == 0) {
+                int stop = 0;
+                if (lane == 0) {
+                    if (lim.deadline_ns && td_globaltimer() > lim.deadline_ns) stop = 1;
+                    if (lim.abort_flag && *(volatile const int *)lim.abort_flag) stop = 1;
+                }
+                if (__shfl_sync(TD_FULL, stop, 0)) {
+                    status = TD_ERR_TIMEOUT;
+                    break;
+                }
+            }
+            const int i = t & 31, j = (t >> 5) & 31, k = (t >> 10) & 31;
+            uint64_t nL;
+            int noff;
+            td_apply_move(s.L[level], s.off[level], N, i, j, k, &nL, &noff);
+            __syncwarp();
+            if (lane == 0) {
+                s.path[level] = (uint16_t)t;
+                s.L[level + 1] = nL;
+                s.off[level + 1] = (uint8_t)noff;
+            }
+            ++level;
+            odd = td_prepare_node(s, nL, noff, N);
+            found = td_evaluate<ORDERED>(s, lut, code, steps, level, odd, maxd);
+            ++expansions;
+        }
+    }
+    __syncwarp();
+    // write the 32-byte result: lanes 0..7 each store one word
+    uint32_t word = 0;
+    if (lane == 0) word = (uint32_t)status;
+    else if (lane == 1) word = (uint32_t)depth;
+    else if (lane >= 2 && lane < 7) {
+        const int m0 = 2 * (lane - 2), m1 = m0 + 1;
+        uint32_t lo = 0, hi = 0;
+        if (status == TD_FOUND) {
+            if (m0 < depth) lo = (m0 == depth - 1) ? found_move : s.path[m0];
+            if (m1 < depth && m1 < TD_MAX_DEPTH) hi = (m1 == depth - 1) ? found_move : s.path[m1];
+        }
+        word = lo | (hi << 16);
+    } else if (lane == 7) {
+        word = expansions;
+    }
+    if (lane < 8) reinterpret_cast<uint32_t *>(out)[lane] = word;
+}

@@ -1,0 +1,108 @@
+"""The engine's warp algorithm, emulated one lane at a time on the host,
+against the oracle: identical witnesses and expansion counts in ordered mode,
+identical verdicts with replayable witnesses in free order."""
+import ctypes as C
+import random
+
+import numpy as np
+import pytest
+
+
+class Inst(C.Structure):
+    _fields_ = [("perm", C.c_uint64), ("min_rate", C.c_float), ("n_symbols", C.c_uint8),
+                ("offset", C.c_uint8), ("max_moves", C.c_uint8), ("packed", C.c_uint8)]
+
+
+class Res(C.Structure):
+    _fields_ = [("status", C.c_int32), ("depth", C.c_int32), ("moves", C.c_uint16 * 9),
+                ("reserved", C.c_uint16), ("expansions", C.c_uint32)]
+
+
+def _u8(v):
+    return (C.c_uint8 * 17)(*v)
+
+
+def _prep(emu, beta, omega, init, rate, maxd, full):
+    x = Inst()
+    rc = emu.td_emu_prepare_pair(_u8(beta), _u8(omega), len(beta), init, C.c_float(rate), maxd, int(full),
+                                 C.byref(x))
+    assert rc == 0
+    return x
+
+
+def _run(emu, x, flags):
+    r = Res()
+    emu.td_emu_search(C.byref(x), flags, C.byref(r))
+    return r, [(m & 31, (m >> 5) & 31, (m >> 10) & 31) for m in r.moves[: r.depth]]
+
+
+def _cases(seed, count):
+    rng = random.Random(seed)
+    for _ in range(count):
+        n = rng.randint(2, 9)
+        pi = list(range(n))
+        rng.shuffle(pi)
+        if rng.random() < 0.25:
+            pi = pi[::-1] if rng.random() < 0.5 else list(range(n))[::-1]
+        yield rng, n, pi
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_ordered_mode_matches_oracle(oracle, emu, seed):
+    for rng, n, pi in _cases(seed, 150):
+        beta, omega, init = oracle.perm_to_pair(pi)
+        N = n + 1
+        r0 = rng.randrange(N)
+        beta = beta[r0:] + beta[:r0]  # general pairs: the array may start anywhere
+        full = rng.random() < 0.8
+        maxd = rng.randint(1, 6)
+        rate = rng.choice([0.0, 1.0, 1.5, 2.0])
+        init_pass = init if full else max(0, init - rng.randint(0, 1))
+        rc, mv, ex = oracle.search(beta, omega, init_pass, rate, maxd, full)
+        x = _prep(emu, beta, omega, init_pass, rate, maxd, full)
+        r, emv = _run(emu, x, 1)
+        assert r.status == rc, (pi, beta, maxd)
+        assert emv == mv, (pi, beta, maxd)
+        assert r.expansions == (ex + 1 if N >= 3 else 0)
+
+
+@pytest.mark.parametrize("seed", [3, 4])
+def test_free_order_verdicts_and_replay(oracle, emu, seed):
+    for rng, n, pi in _cases(seed, 150):
+        beta, omega, init = oracle.perm_to_pair(pi)
+        maxd = rng.randint(1, 6)
+        rc, _, _ = oracle.search(beta, omega, init, 0.0, maxd, True)
+        x = _prep(emu, beta, omega, init, 0.0, maxd, True)
+        r, emv = _run(emu, x, 0)
+        assert r.status == rc
+        if rc == 1:
+            abc = oracle.positions_to_symbols(beta, emv)
+            assert oracle.validate(beta, omega, abc, maxd) is None
+
+
+def test_pinned_move_matches_block_swap(oracle, emu):
+    """td_apply_move on the pinned state equals the block swap of the caller's
+    array, including the new array start when i == 0."""
+    rng = random.Random(5)
+    for _ in range(400):
+        n = rng.randint(3, 17)
+        N = n
+        pi = list(range(n - 1))
+        rng.shuffle(pi)
+        beta, omega, init = oracle.perm_to_pair(pi)
+        r0 = rng.randrange(N)
+        beta = beta[r0:] + beta[:r0]
+        x = _prep(emu, beta, omega, init, 0.0, 9, True)
+        L, off = x.perm, x.offset
+        cur = list(beta)
+        B = [0] + [((L >> (4 * m)) & 15) + 1 for m in range(N - 1)]
+        sigma = {a: B[(p + off) % N] for p, a in enumerate(cur)}  # the instance's fixed relabeling
+        assert len(set(sigma.values())) == N
+        for _ in range(4):
+            i, j, k = sorted(rng.sample(range(N), 3))
+            outL, outOff = C.c_uint64(), C.c_int()
+            emu.td_emu_apply_move(C.c_uint64(L), off, N, i, j, k, C.byref(outL), C.byref(outOff))
+            L, off = outL.value, outOff.value
+            cur = cur[:i] + cur[j:k] + cur[i:j] + cur[k:]
+            B = [0] + [((L >> (4 * m)) & 15) + 1 for m in range(N - 1)]
+            assert [B[(p + off) % N] for p in range(N)] == [sigma[a] for a in cur]

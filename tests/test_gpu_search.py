@@ -1,0 +1,181 @@
+"""Parity of the CUDA search with the oracle, through the C ABI (needs a B200)."""
+import concurrent.futures as cf
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ORDERED, PLAIN = 1, 2
+MiB = 1 << 20
+
+
+@pytest.fixture(scope="module")
+def slots(td):
+    td.init_slots(2, [0], 64 * MiB)
+    yield td
+    td.destroy()
+
+
+def _pairs(oracle, perms, n):
+    c = len(perms)
+    beta = np.zeros((c, 17), np.uint8)
+    omega = np.zeros((c, 17), np.uint8)
+    init = np.zeros(c, np.int32)
+    N = np.zeros(c, np.uint8)
+    for i, (p, k) in enumerate(zip(perms, n)):
+        b, o, e = oracle.perm_to_pair(p[:k].tolist())
+        beta[i, : k + 1] = b
+        omega[i, : k + 1] = o
+        init[i] = e
+        N[i] = k + 1
+    return beta, omega, init, N
+
+
+def _oracle_batch(oracle, beta, omega, N, init, rate, maxd, full):
+    c = len(N)
+    return oracle.search_batch(beta, omega, N, init, np.broadcast_to(rate, (c,)).astype(np.float32),
+                               np.broadcast_to(maxd, (c,)).astype(np.int32),
+                               np.broadcast_to(full, (c,)).astype(np.uint8), os.cpu_count() or 8)
+
+
+def _replay_all(oracle, beta, omega, N, res, maxd):
+    for i in np.nonzero(res["status"] == 1)[0]:
+        k = int(N[i])
+        moves = [(int(m) & 31, (int(m) >> 5) & 31, (int(m) >> 10) & 31) for m in res["moves"][i][: res["depth"][i]]]
+        abc = oracle.positions_to_symbols(beta[i, :k].tolist(), moves)
+        err = oracle.validate(beta[i, :k].tolist(), omega[i, :k].tolist(), abc, int(np.broadcast_to(maxd, (len(N),))[i]))
+        assert err is None, (i, err)
+
+
+def test_smoke_concurrent_three_cycles_through_the_slot_queue(td):
+    """GPUSortingSearchSmokeTest: 2 slots, 32 MiB, 32 concurrent N=3 searches."""
+    td.GPUSortingSearch.init([0], 2, 32 * MiB, queue_capacity=0)
+    try:
+        inst = td.GPUSortingSearch.get_instance()
+        with cf.ThreadPoolExecutor(32) as ex:
+            futs = [ex.submit(inst.search, bytes([0, 1, 2]), bytes([1, 2, 0]), 1, 2.0, 1, True) for _ in range(32)]
+            for f in futs:
+                assert f.result() == [(0, 1, 2)]
+        snap = inst.stats.snapshot(__import__("time").monotonic_ns())
+        assert snap.completed == 32 and snap.failed == 0
+    finally:
+        td.GPUSortingSearch.shutdown()
+
+
+def test_config1_exact_distance_and_ordered_witnesses(slots, oracle):
+    """4096 x S_10 from seed 0: deepening the bound gives the exact restricted
+    distance; each witness is the reference single-queue witness."""
+    td = slots
+    perms, n = td.synth_perms(0, 4096, 10, 10, 0, 0, 0)
+    beta, omega, init, N = _pairs(oracle, perms, n)
+    dist_gpu = np.full(4096, -1)
+    dist_ora = np.full(4096, -1)
+    for d in range(1, 7):
+        inst = td.prepare_pairs(beta, omega, N, init, 0.0, d, 1)
+        res, _ = td.search_batch(0, inst, ORDERED)
+        st, dep, mv, ex = _oracle_batch(oracle, beta, omega, N, init, 0.0, d, 1)
+        assert (res["status"] == st).all()
+        assert (res["depth"] == dep).all()
+        assert (res["moves"] == mv).all()
+        assert (res["expansions"] == ex + 1).all()
+        dist_gpu[(dist_gpu < 0) & (res["status"] == 1)] = d
+        dist_ora[(dist_ora < 0) & (st == 1)] = d
+    assert (dist_gpu == dist_ora).all() and dist_gpu.max() == 6 and (dist_gpu > 0).all()
+
+
+def test_ordered_general_pairs_rates_and_partial_sorting(slots, oracle):
+    td = slots
+    rng = np.random.default_rng(7)
+    c = 1500
+    perms, n = td.synth_perms(11, c, 4, 11, 20, 1, 3)
+    beta, omega, init, N = _pairs(oracle, perms, n)
+    for i in range(c):  # rotate the caller's array to exercise betaStart
+        k = int(N[i])
+        r = int(rng.integers(k))
+        beta[i, :k] = np.roll(beta[i, :k], -r)
+    maxd = rng.integers(1, 7, c).astype(np.int32)
+    rate = rng.choice([0.0, 1.0, 1.5, 2.0], c).astype(np.float32)
+    full = (rng.random(c) < 0.7).astype(np.uint8)
+    init_pass = np.where(full == 1, init, np.maximum(0, init - rng.integers(0, 2, c))).astype(np.int32)
+    inst = td.prepare_pairs(beta, omega, N, init_pass, rate, maxd, full)
+    res, _ = td.search_batch(1, inst, ORDERED)
+    st, dep, mv, ex = _oracle_batch(oracle, beta, omega, N, init_pass, rate, maxd, full)
+    assert (res["status"] == st).all()
+    assert (res["depth"] == dep).all() and (res["moves"] == mv).all()
+    assert (res["expansions"] == np.where(N >= 3, ex + 1, 0)).all()
+
+
+def test_config2_mix_free_order_verdicts_and_replay(slots, oracle):
+    """Sample of the batched uneven mix: n in {11,12,13}, 25% near-reverse,
+    bound floor(n/2)+1.  Verdicts equal the oracle's; every witness replays."""
+    td = slots
+    perms, n = td.synth_perms(1, 4096, 11, 13, 25, 1, 3)
+    beta, omega, init, N = _pairs(oracle, perms, n)
+    maxd = (n // 2 + 1).astype(np.int32)
+    inst = td.prepare_pairs(beta, omega, N, init, 0.0, maxd, 1)
+    res, stats = td.search_batch(0, inst, 0)
+    st, _, _, _ = _oracle_batch(oracle, beta, omega, N, init, 0.0, maxd, 1)
+    assert (res["status"] == st).all()
+    assert stats.found + stats.not_found == 4096 and stats.errors == 0
+    _replay_all(oracle, beta, omega, N, res, maxd)
+    res_p, _ = td.search_batch(0, inst, PLAIN)
+    assert (res_p["status"] == res["status"]).all()
+
+
+def test_config3_s16_witnesses_replay_and_verdict_sample(slots, oracle):
+    """S_16, bound 9, half uniform and half near-reverse."""
+    td = slots
+    perms, n = td.synth_perms(2, 1 << 14, 16, 16, 50, 1, 4)
+    inst = td.prepare_perms(perms, n, 9)
+    res, stats = td.search_batch(0, inst, 0)
+    assert stats.errors == 0
+    beta, omega, init, N = _pairs(oracle, perms[:192], n[:192])
+    st, _, _, _ = _oracle_batch(oracle, beta, omega, N, init, 0.0, 9, 1)
+    assert (res["status"][:192] == st).all()
+    sample = np.arange(0, 1 << 14, 7)
+    b2, o2, _, N2 = _pairs(oracle, perms[sample], n[sample])
+    _replay_all(oracle, b2, o2, N2, res[sample], 9)
+
+
+def test_device_entry_points_with_validator(slots):
+    import torch
+    td = slots
+    perms, n = td.synth_perms(2, 8192, 16, 16, 50, 1, 4)
+    inst = td.prepare_perms(perms, n, 9)
+    d_in = torch.from_numpy(inst.view(np.uint8).copy()).cuda()
+    d_out = torch.zeros(8192 * 32, dtype=torch.uint8, device="cuda")
+    d_ok = torch.zeros(8192, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    td._lib.search_batch_device(0, 8192, d_in.data_ptr(), d_out.data_ptr(), 0, 0, stream)
+    td._lib.validate_batch_device(8192, d_in.data_ptr(), d_out.data_ptr(), d_ok.data_ptr(), stream)
+    torch.cuda.synchronize()
+    res = d_out.cpu().numpy().view(td.RESULT_DTYPE)
+    ok = d_ok.cpu().numpy()
+    assert ((res["status"] == 1) == (ok == 1)).all()
+    host_res, _ = td.search_batch(0, inst, 0)
+    assert (host_res["status"] == res["status"]).all()
+
+
+def test_edge_cases(slots):
+    td = slots
+    assert td.search(0, b"", b"", 0, 0.0, 1) == []
+    assert td.search(0, bytes([0, 1]), bytes([1, 0]), 0, 0.0, 1) == []
+    assert td.search(0, bytes([0, 1, 2]), bytes([1, 2, 0]), 1, 2.0, 1, ordered=True) == [(0, 1, 2)]
+    # identity omega: every symbol fixed, no move applies
+    assert td.search(0, bytes([0, 1, 2, 3]), bytes([0, 1, 2, 3]), 4, 0.0, 3) == []
+    for bad in (dict(max_moves=0), dict(max_moves=10)):
+        with pytest.raises(td.TdError):
+            td.search(0, bytes([0, 1, 2]), bytes([1, 2, 0]), 1, 2.0, bad["max_moves"])
+    with pytest.raises(td.TdError):
+        td.search(0, bytes(range(18)), bytes(range(18)), 0, 0.0, 1)
+    with pytest.raises(td.TdError):
+        td.search(5, bytes([0, 1, 2]), bytes([1, 2, 0]), 1, 2.0, 1)
+    with pytest.raises(td.TdError):
+        td.search(0, bytes([0, 1, 1]), bytes([1, 2, 0]), 1, 2.0, 1)
+    # a work budget that is too small reports the reference's overflow class
+    perms, n = td.synth_perms(2, 64, 16, 16, 100, 1, 1)
+    inst = td.prepare_perms(perms, n, 9)
+    res, _ = td.search_batch(0, inst, ORDERED, max_expansions=2)
+    assert (res["status"] == -2).any()
