@@ -71,6 +71,9 @@ typedef struct td_batch_stats {
     uint64_t not_found;    /* instances exhausted */
     uint64_t errors;       /* instances with status < 0 */
     float kernel_ms;       /* device time of the search launch(es) */
+    uint32_t launches;     /* reserved */
+    uint64_t donations;    /* free-order engine: donation events */
+    uint64_t donated_items;/* free-order engine: subtrees handed between warps */
 } td_batch_stats;
 
 /* ---- slots: the reference's JNI boundary --------------------------------- */
@@ -108,6 +111,13 @@ int td_slot_count(void);
 int td_slot_device(int slot);           /* -1 for an invalid slot */
 void *td_slot_stream(int slot);         /* cudaStream_t of the slot */
 int td_destroy(void);                   /* releases every slot */
+
+/* Launch shape of the engine (the autotuner's knobs): warps per block and
+ * instances per ticket of the ordered persistent kernel. */
+int td_configure(int warps_per_block, int grain);
+/* Work donation of the free-order engine: items per donation, deepest level
+ * whose children may be donated, expansions between idle checks. */
+int td_configure_steal(int grain, int split_level, int check_every);
 
 /* ---- instance preparation (host, no GPU needed) -------------------------- */
 

@@ -27,7 +27,8 @@ assert INSTANCE_DTYPE.itemsize == 16 and RESULT_DTYPE.itemsize == 32
 
 class BatchStats(C.Structure):
     _fields_ = [("expansions", C.c_uint64), ("found", C.c_uint64), ("not_found", C.c_uint64),
-                ("errors", C.c_uint64), ("kernel_ms", C.c_float)]
+                ("errors", C.c_uint64), ("kernel_ms", C.c_float), ("launches", C.c_uint32),
+                ("donations", C.c_uint64), ("donated_items", C.c_uint64)]
 
 
 class TdError(RuntimeError):
@@ -41,7 +42,7 @@ _lib = None
 EXPORTS = ["td_init_slots", "td_search", "td_search_ordered", "td_slot_count", "td_slot_device",
            "td_slot_stream", "td_destroy", "td_prepare_pairs", "td_prepare_perms", "td_synth_perms",
            "td_search_batch", "td_search_batch_device", "td_validate_batch_device",
-           "td_positions_to_symbols", "td_configure", "td_int_issue_peak"]
+           "td_positions_to_symbols", "td_configure", "td_configure_steal", "td_int_issue_peak"]
 
 
 def lib():
@@ -72,6 +73,7 @@ def lib():
     L.td_positions_to_symbols.argtypes = [vp, C.c_int, vp, C.c_int, vp]
     L.td_positions_to_symbols.restype = None
     L.td_configure.argtypes = [C.c_int, C.c_int]
+    L.td_configure_steal.argtypes = [C.c_int, C.c_int, C.c_int]
     _lib = L
     return L
 
@@ -197,6 +199,11 @@ def positions_to_symbols(beta, moves):
 def configure(warps_per_block: int, grain: int) -> None:
     if lib().td_configure(int(warps_per_block), int(grain)) != OK:
         raise TdError(INVALID_ARG, "invalid launch configuration")
+
+
+def configure_steal(grain: int, split_level: int, check_every: int) -> None:
+    if lib().td_configure_steal(int(grain), int(split_level), int(check_every)) != OK:
+        raise TdError(INVALID_ARG, "invalid donation parameters")
 
 
 def unpack_moves(row) -> list:

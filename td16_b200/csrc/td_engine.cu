@@ -38,6 +38,8 @@
 struct td_batch_stats {
     uint64_t expansions, found, not_found, errors;
     float kernel_ms;
+    uint32_t launches;
+    uint64_t donations, donated_items;
 };
 
 static_assert(sizeof(td_instance) == 16, "td_instance layout");
@@ -109,6 +111,179 @@ __global__ void __launch_bounds__(256) td_persistent_kernel(const td_instance *_
     }
 }
 
+// Resident grid with work donation (free move order).  Warps take fresh
+// instances by ticket; a warp that finds neither tickets nor items counts
+// itself idle, and busy warps then hand the remaining children of their
+// shallowest DFS level to the item array.  Every wait is bounded by the
+// launch deadline; the launch ends when no ticket, item or unit is left.
+__device__ __forceinline__ void td_finish_unit(const td_dfs_out &r, td_inst_state *st, td_result *out,
+                                               const uint16_t *path) {
+    const int lane = threadIdx.x & 31;
+    int win = 0, last = 0;
+    if (lane == 0) {
+        atomicAdd(&st->expansions, r.expansions);
+        if (r.status == TD_DFS_FOUND) win = atomicCAS(&st->found, 0, 1) == 0;
+        if (r.status == TD_DFS_TIMEOUT) atomicCAS(&st->error, 0, TD_ERR_TIMEOUT);
+    }
+    win = __shfl_sync(TD_FULL, win, 0);
+    if (win) td_write_result(out, TD_FOUND, r.depth, r.found_move, path, 0, 0, 7);
+    __syncwarp();
+    if (lane == 0) {
+        __threadfence();
+        last = atomicSub(&st->pending, 1) == 1;
+        if (last) __threadfence();
+    }
+    last = __shfl_sync(TD_FULL, last, 0);
+    if (last) {
+        int found = 0, err = 0;
+        unsigned exp = 0;
+        if (lane == 0) {
+            found = *(volatile int *)&st->found;
+            err = *(volatile int *)&st->error;
+            exp = *(volatile unsigned *)&st->expansions;
+        }
+        found = __shfl_sync(TD_FULL, found, 0);
+        err = __shfl_sync(TD_FULL, err, 0);
+        exp = __shfl_sync(TD_FULL, exp, 0);
+        if (!found) td_write_result(out, err ? err : TD_NOT_FOUND, 0, 0, path, exp, 0, 8);
+        else td_write_result(out, TD_FOUND, 0, 0, path, exp, 7, 8);
+    }
+}
+
+__global__ void __launch_bounds__(256) td_steal_kernel(const td_instance *__restrict__ in,
+                                                      td_result *__restrict__ out, int count, td_pool *pool,
+                                                      td_item *items, uint32_t *ready, uint32_t epoch,
+                                                      int capacity, td_inst_state *state, int grain,
+                                                      int max_level, int check_every, uint64_t time_limit_ns) {
+    extern __shared__ __align__(16) uint8_t td_smem[];
+    const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint8_t *lut = td_smem;
+    td_warp_smem *ws = reinterpret_cast<td_warp_smem *>(td_smem + TD_LUT_BYTES);
+    td_block_init(lut, ws, warps);
+    td_warp_smem &s = ws[warp];
+    uint32_t code[TD_MAX_STEPS];
+    int codeN = -1;
+    td_search_limits lim = td_make_limits(0, time_limit_ns, nullptr);
+    td_donate_ctx dc;
+    dc.pool = pool;
+    dc.items = items;
+    dc.ready = ready;
+    dc.epoch = epoch;
+    dc.capacity = capacity;
+    dc.grain = grain;
+    dc.max_level = max_level;
+    dc.check_every = check_every > 0 ? check_every : 1;
+    bool idle = false;
+    unsigned backoff = 64;
+    for (;;) {
+        int kind = 0, unit = -1;
+        if (lane == 0) {
+            atomicAdd(&pool->active, 1);
+            if (*(volatile int *)&pool->inst_ticket < count) {
+                const int t = atomicAdd(&pool->inst_ticket, 1);
+                if (t < count) { kind = 1; unit = t; }
+            }
+            if (!kind) {
+                const int P = *(volatile int *)&pool->produced;
+                int C = *(volatile int *)&pool->consumed;
+                while (C < P) {
+                    const int prev = atomicCAS(&pool->consumed, C, C + 1);
+                    if (prev == C) { kind = 2; unit = C; break; }
+                    C = prev;
+                }
+            }
+            if (!kind) atomicSub(&pool->active, 1);
+        }
+        kind = __shfl_sync(TD_FULL, kind, 0);
+        unit = __shfl_sync(TD_FULL, unit, 0);
+        if (!kind) {
+            int done = 0;
+            if (lane == 0) {
+                const int tk = *(volatile int *)&pool->inst_ticket;
+                const int ac = *(volatile int *)&pool->active;
+                const int pr = *(volatile int *)&pool->produced;
+                const int co = *(volatile int *)&pool->consumed;
+                done = tk >= count && ac == 0 && co >= pr;
+                if (!done && !idle) { atomicAdd(&pool->idle, 1); idle = true; }
+                if (!done && lim.deadline_ns && td_globaltimer() > lim.deadline_ns) {
+                    atomicCAS(&pool->error, 0, TD_ERR_TIMEOUT);
+                    done = 1;
+                }
+            }
+            if (__shfl_sync(TD_FULL, done, 0)) break;
+            __nanosleep(backoff);
+            backoff = min(backoff * 2u, 8192u);
+            continue;
+        }
+        if (lane == 0 && idle) { atomicSub(&pool->idle, 1); idle = false; }
+        backoff = 64;
+        if (kind == 1) {
+            const td_instance x = in[unit];
+            td_inst_state *st = &state[unit];
+            if (!td_instance_ok(x) || td_triple_count(x.n_symbols) == 0) {
+                td_write_result(&out[unit], td_instance_ok(x) ? TD_NOT_FOUND : TD_ERR_ARG, 0, 0, s.path, 0, 0, 8);
+            } else {
+                if (lane == 0) atomicAdd(&st->pending, 1);
+                td_setup_root(s, x, code, codeN);
+                dc.inst = (uint32_t)unit;
+                dc.state = st;
+                const td_dfs_out r = td_dfs<false>(s, lut, code, x.n_symbols, x.max_moves, 0, lim, &dc);
+                td_finish_unit(r, st, &out[unit], s.path);
+            }
+        } else {
+            // wait until the donor has written the item (bounded)
+            int ok = 0;
+            if (lane == 0) {
+                for (unsigned spin = 0; spin < (1u << 30); ++spin) {
+                    if (*(volatile uint32_t *)&ready[unit] == epoch) { ok = 1; break; }
+                    if ((spin & 1023u) == 0 && lim.deadline_ns && td_globaltimer() > lim.deadline_ns) break;
+                    __nanosleep(32);
+                }
+                if (!ok) atomicCAS(&pool->error, 0, TD_ERR_TIMEOUT);
+                __threadfence();
+            }
+            ok = __shfl_sync(TD_FULL, ok, 0);
+            if (ok) {
+                td_item it;  // read through L2: the donor wrote it from another SM
+                {
+                    const uint4 *src = reinterpret_cast<const uint4 *>(&items[unit]);
+                    uint4 *dst = reinterpret_cast<uint4 *>(&it);
+                    dst[0] = __ldcg(src);
+                    dst[1] = __ldcg(src + 1);
+                }
+                const uint32_t idx = it.inst;
+                const td_instance x = in[idx];
+                td_inst_state *st = &state[idx];
+                td_setup_root(s, x, code, codeN);
+                const int d0 = it.depth;
+                if (lane == 0) {
+                    s.L[d0] = it.L;
+                    s.off[d0] = it.off;
+                    for (int d = 0; d < d0; ++d) s.path[d] = it.path[d];
+                }
+                __syncwarp();
+                int stop = 0;
+                if (lane == 0) stop = *(volatile int *)&st->found;
+                stop = __shfl_sync(TD_FULL, stop, 0);
+                td_dfs_out r;
+                if (stop) {
+                    r.status = TD_DFS_ABORTED;
+                    r.depth = 0;
+                    r.found_move = 0;
+                    r.expansions = 0;
+                } else {
+                    dc.inst = idx;
+                    dc.state = st;
+                    r = td_dfs<false>(s, lut, code, x.n_symbols, x.max_moves, d0, lim, &dc);
+                }
+                td_finish_unit(r, st, &out[idx], s.path);
+            }
+        }
+        if (lane == 0) atomicSub(&pool->active, 1);
+    }
+    if (lane == 0 && idle) atomicSub(&pool->idle, 1);
+}
+
 // Witness replay in pinned form: every move must be an in-range position
 // triple i<j<k, at most max_moves of them, and the final state must be the
 // identity (omega = id  <=>  beta = rho  <=>  L = 0,1,...,n-1).
@@ -178,6 +353,14 @@ struct Slot {
     int *d_ticket = nullptr;
     void *d_batch = nullptr;
     size_t d_batch_bytes = 0;
+    // donation scratch: pool counters, item array + ready flags, instance state
+    td_pool *d_pool = nullptr;
+    td_item *d_items = nullptr;
+    uint32_t *d_ready = nullptr;
+    int item_capacity = 0;
+    td_inst_state *d_state = nullptr;
+    size_t state_count = 0;
+    uint32_t epoch = 0;
     std::mutex *mu = nullptr;
 };
 
@@ -185,6 +368,7 @@ struct DeviceInfo {
     bool ready = false;
     int sms = 0;
     int blocks_per_sm = 0;
+    int steal_blocks_per_sm = 0;
 };
 
 std::mutex g_mu;
@@ -192,7 +376,10 @@ std::vector<Slot> g_slots;
 std::vector<DeviceInfo> g_dev;
 
 int g_warps_per_block = 4;
-int g_grain = 1;
+int g_grain = 1;            // instances per ticket (ordered persistent kernel)
+int g_steal_grain = 4;      // items per donation
+int g_split_level = 4;      // donate children of levels <= this
+int g_check_every = 8;      // expansions between idle checks
 
 void set_err(char *err, size_t len, const std::string &msg) {
     if (err && len) {
@@ -246,6 +433,7 @@ int ensure_device(int device, char *err, size_t errlen) {
     TD_CHECK(cudaFuncSetAttribute(td_plain_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
     TD_CHECK(cudaFuncSetAttribute(td_persistent_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
     TD_CHECK(cudaFuncSetAttribute(td_persistent_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
+    TD_CHECK(cudaFuncSetAttribute(td_steal_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
     d.ready = true;
     return TD_OK;
 }
@@ -257,6 +445,10 @@ void release_slot(Slot &s) {
     if (s.d_res) cudaFree(s.d_res);
     if (s.d_ticket) cudaFree(s.d_ticket);
     if (s.d_batch) cudaFree(s.d_batch);
+    if (s.d_pool) cudaFree(s.d_pool);
+    if (s.d_items) cudaFree(s.d_items);
+    if (s.d_ready) cudaFree(s.d_ready);
+    if (s.d_state) cudaFree(s.d_state);
     if (s.h_inst) cudaFreeHost(s.h_inst);
     if (s.h_res) cudaFreeHost(s.h_res);
     if (s.done) cudaEventDestroy(s.done);
@@ -284,6 +476,40 @@ int launch_batch(Slot &s, int count, const td_instance *d_in, td_result *d_out, 
         const int blocks = (count + warps - 1) / warps;
         if (ordered) td_plain_kernel<true><<<blocks, threads, smem, stream>>>(d_in, d_out, count, max_exp, time_limit_ns());
         else td_plain_kernel<false><<<blocks, threads, smem, stream>>>(d_in, d_out, count, max_exp, time_limit_ns());
+    } else if (!ordered) {
+        // item space: the slot budget (the reference's queue budget) less the
+        // per-instance state, at 36 bytes per item (record + ready flag)
+        if (s.d_pool == nullptr) {
+            TD_CHECK(cudaMalloc(&s.d_pool, sizeof(td_pool)));
+            const size_t cap = std::max<size_t>(1024, std::min<size_t>(s.budget / 36, 1u << 26));
+            TD_CHECK(cudaMalloc(&s.d_items, cap * sizeof(td_item)));
+            TD_CHECK(cudaMalloc(&s.d_ready, cap * sizeof(uint32_t)));
+            TD_CHECK(cudaMemset(s.d_ready, 0, cap * sizeof(uint32_t)));
+            s.item_capacity = (int)cap;
+        }
+        if ((size_t)count > s.state_count) {
+            if (s.d_state) TD_CHECK(cudaFree(s.d_state));
+            s.d_state = nullptr;
+            s.state_count = 0;
+            TD_CHECK(cudaMalloc(&s.d_state, (size_t)count * sizeof(td_inst_state)));
+            s.state_count = (size_t)count;
+        }
+        if (++s.epoch == 0) {  // ready flags from 2^32 launches ago could alias
+            TD_CHECK(cudaMemsetAsync(s.d_ready, 0, (size_t)s.item_capacity * sizeof(uint32_t), stream));
+            s.epoch = 1;
+        }
+        DeviceInfo &d = g_dev[s.device];
+        if (d.steal_blocks_per_sm == 0) {
+            int b = 0;
+            TD_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, td_steal_kernel, threads, smem));
+            d.steal_blocks_per_sm = std::max(1, b);
+        }
+        const int grid = std::max(1, std::min(d.sms * d.steal_blocks_per_sm, (count + warps - 1) / warps));
+        TD_CHECK(cudaMemsetAsync(s.d_pool, 0, sizeof(td_pool), stream));
+        TD_CHECK(cudaMemsetAsync(s.d_state, 0, (size_t)count * sizeof(td_inst_state), stream));
+        td_steal_kernel<<<grid, threads, smem, stream>>>(d_in, d_out, count, s.d_pool, s.d_items, s.d_ready, s.epoch,
+                                                         s.item_capacity, s.d_state, g_steal_grain, g_split_level,
+                                                         g_check_every, time_limit_ns());
     } else {
         DeviceInfo &d = g_dev[s.device];
         if (d.blocks_per_sm == 0) {
@@ -541,7 +767,18 @@ TD_API int td_configure(int warps_per_block, int grain) {
     std::lock_guard<std::mutex> g(g_mu);
     g_warps_per_block = warps_per_block;
     g_grain = grain;
-    for (auto &d : g_dev) d.blocks_per_sm = 0;
+    for (auto &d : g_dev) d.blocks_per_sm = d.steal_blocks_per_sm = 0;
+    return TD_OK;
+}
+
+// Work-donation parameters of the free-order engine: items per donation,
+// deepest level whose children may be donated, expansions between checks.
+TD_API int td_configure_steal(int grain, int split_level, int check_every) {
+    if (grain < 1 || split_level < 0 || split_level >= TD_MAX_DEPTH || check_every < 1) return TD_INVALID_ARG;
+    std::lock_guard<std::mutex> g(g_mu);
+    g_steal_grain = grain;
+    g_split_level = split_level;
+    g_check_every = check_every;
     return TD_OK;
 }
 
@@ -676,6 +913,16 @@ TD_API int td_search_batch(int slot, int count, const td_instance *in, td_result
     if (stats) {
         std::memset(stats, 0, sizeof *stats);
         TD_CHECK(cudaEventElapsedTime(&stats->kernel_ms, s->t0, s->t1));
+        if (!(flags & (TD_FLAG_ORDERED | TD_FLAG_PLAIN)) && s->d_pool) {
+            td_pool pool;
+            TD_CHECK(cudaMemcpy(&pool, s->d_pool, sizeof pool, cudaMemcpyDeviceToHost));
+            stats->donations = pool.donations;
+            stats->donated_items = pool.donated_items;
+            if (pool.error) {
+                set_err(err, errlen, "engine launch deadline reached");
+                return TD_TIMEOUT;
+            }
+        }
         for (int i = 0; i < count; ++i) {
             stats->expansions += out[i].expansions;
             if (out[i].status == TD_FOUND) stats->found++;

@@ -62,7 +62,7 @@ __device__ __forceinline__ void td_load_codes(int N, uint32_t (&code)[TD_MAX_STE
 __device__ __forceinline__ int td_prepare_node(td_warp_smem &s, uint64_t L, int off, int N) {
     const int p = threadIdx.x & 31;
     const bool act = p < N;
-    const uint32_t Bp = p == 0 ? 0u : td_nib(L, p - 1) + 1u;
+    const uint32_t Bp = (p == 0 || !act) ? 0u : td_nib(L, p - 1) + 1u;
     // inverse of L by a warp OR of one nibble per lane
     uint32_t lo = 0, hi = 0;
     if (p < N - 1) {
@@ -245,93 +245,248 @@ __device__ __forceinline__ int td_next_child(td_warp_smem &s, int level, int *ac
     return st * 32 + win;
 }
 
-// One complete search by the calling warp.  `code`/`codeN` cache the lane's
-// triple offsets for the last N seen.  Writes *out from lane 0.
-template <bool ORDERED>
-__device__ void td_warp_search(const td_instance &x, td_result *out, td_warp_smem &s,
-                               const uint8_t *lut, uint32_t (&code)[TD_MAX_STEPS], int &codeN,
-                               const td_search_limits &lim) {
+// ---- work items (subtree roots handed between warps) ----------------------
+
+// A node that is known to be expandable, with the moves that lead to it.
+struct __align__(16) td_item {  // 32 bytes
+    uint64_t L;
+    uint32_t inst;          // instance index
+    uint8_t depth;          // >= 1
+    uint8_t off;
+    uint16_t path[TD_MAX_DEPTH];
+};
+
+// Per-instance bookkeeping when several warps share one search.
+struct td_inst_state {
+    int found;              // set once by the warp that records the witness
+    int pending;            // units (the root search + items) not yet finished
+    unsigned expansions;    // summed over units
+    int error;              // first error status seen (timeout)
+};
+
+// Scheduler counters of one launch.
+struct td_pool {
+    int inst_ticket;        // next fresh instance
+    int produced;           // items reserved by donors
+    int consumed;           // items claimed by takers
+    int active;             // warps inside a unit or claiming one
+    int idle;               // warps waiting for donated work
+    int error;              // launch-level error (bounded wait expired)
+    unsigned long long donations;
+    unsigned long long donated_items;
+};
+
+struct td_donate_ctx {
+    td_pool *pool;
+    td_item *items;
+    uint32_t *ready;        // ready[i] == epoch once item i is written
+    uint32_t epoch;
+    int capacity;
+    int grain;              // at most this many items per donation
+    int max_level;          // donate only children of levels <= max_level
+    int check_every;        // expansions between idle checks
+    uint32_t inst;
+    td_inst_state *state;
+};
+
+#define TD_DFS_FOUND 1
+#define TD_DFS_EXHAUSTED 0
+#define TD_DFS_BUDGET (-2)
+#define TD_DFS_TIMEOUT (-5)
+#define TD_DFS_ABORTED (-7)
+
+struct td_dfs_out {
+    int status;
+    int depth;
+    uint16_t found_move;
+    uint32_t expansions;
+};
+
+// Hands some remaining children of the shallowest level in [d0, level] to the
+// pool as items.  Returns the number donated (uniform across the warp).
+__device__ __forceinline__ int td_donate(td_warp_smem &s, const td_donate_ctx &dc, int d0, int level, int N,
+                                         int T, int tri_base, int want) {
     const int lane = threadIdx.x & 31;
-    const int N = x.n_symbols;
-    const int maxd = x.max_moves;
+    int lv = -1;
+    for (int l = d0; l <= level && l <= dc.max_level; ++l) {
+        const uint32_t w = s.m1[l][lane] | s.m2[l][lane];
+        if (__any_sync(TD_FULL, w != 0)) { lv = l; break; }
+    }
+    if (lv < 0) return 0;
+    // leave at least one child to this warp when the level is the current one
+    uint32_t w1 = s.m1[lv][lane], w2 = s.m2[lv][lane];
+    const int have = __reduce_add_sync(TD_FULL, (unsigned)(__popc(w1) + __popc(w2)));
+    int give = min(want, have - (lv == level ? 1 : 0));
+    if (give <= 0) return 0;
+    // take the lowest lanes' bits first: lane l gives up to `mine` children
+    const int cnt = __popc(w1) + __popc(w2);
+    int before = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(TD_FULL, before, o);
+        if (lane >= o) before += v;
+    }
+    before -= cnt;  // exclusive prefix
+    const int mine = max(0, min(cnt, give - before));
+    // reserve `give` item slots; the count never passes the capacity and never
+    // goes back, so a taker only ever claims slots that a donor will write
+    int base = -1;
+    if (lane == 0) {
+        int cur = *(volatile int *)&dc.pool->produced;
+        while (cur + give <= dc.capacity) {
+            const int prev = atomicCAS(&dc.pool->produced, cur, cur + give);
+            if (prev == cur) { base = cur; break; }
+            cur = prev;
+        }
+        // the pending count must cover the items before any taker can finish one
+        if (base >= 0) atomicAdd(&dc.state->pending, give);
+        __threadfence();
+    }
+    base = __shfl_sync(TD_FULL, base, 0);
+    if (base < 0) return 0;  // out of item space: keep the work
+    if (lane == 0) {
+        atomicAdd(&dc.pool->donations, 1ull);
+        atomicAdd(&dc.pool->donated_items, (unsigned long long)give);
+    }
+    int slot = base + before;
+    for (int taken = 0; taken < mine; ++taken) {
+        uint32_t *wp = w1 ? &w1 : &w2;
+        const int st = __ffs(*wp) - 1;
+        *wp &= *wp - 1;
+        const int u = 32 * st + lane;
+        const uint32_t t = td_tri_table[tri_base + T - 1 - u];
+        uint64_t nL;
+        int noff;
+        td_apply_move(s.L[lv], s.off[lv], N, t & 31, (t >> 5) & 31, (t >> 10) & 31, &nL, &noff);
+        td_item it;
+        it.L = nL;
+        it.inst = dc.inst;
+        it.depth = (uint8_t)(lv + 1);
+        it.off = (uint8_t)noff;
+#pragma unroll
+        for (int d = 0; d < TD_MAX_DEPTH; ++d) it.path[d] = d < lv ? s.path[d] : (d == lv ? (uint16_t)t : 0);
+        dc.items[slot] = it;
+        __threadfence();
+        atomicExch(&dc.ready[slot], dc.epoch);
+        ++slot;
+    }
+    s.m1[lv][lane] = w1;
+    s.m2[lv][lane] = w2;
+    __syncwarp();
+    return give;
+}
+
+// Depth-first search from the node held at level d0 of `s` (state, path and
+// rate masks already set).  Leaves the frames intact on TD_DFS_BUDGET.
+template <bool ORDERED>
+__device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t (&code)[TD_MAX_STEPS],
+                             int N, int maxd, int d0, const td_search_limits &lim, const td_donate_ctx *dc) {
+    const int lane = threadIdx.x & 31;
     const int T = td_triple_count(N);
-    int status = TD_NOT_FOUND, depth = 0;
-    uint32_t expansions = 0;
-    uint16_t found_move = 0;
-    if (N > TD_MAX_N || maxd < 1 || maxd > TD_MAX_DEPTH || td_inst_init(x) > TD_MAX_N) {
-        status = TD_ERR_ARG;
-    } else if (T > 0) {
-        if (codeN != N) {
-            td_load_codes(N, code);
-            codeN = N;
+    const int steps = (T + 31) >> 5;
+    const int tri_base = td_tri_base(N);
+    td_dfs_out r;
+    r.status = TD_DFS_EXHAUSTED;
+    r.depth = 0;
+    r.found_move = 0;
+    r.expansions = 0;
+    int level = d0;
+    int odd = td_prepare_node(s, s.L[d0], s.off[d0], N);
+    int found = td_evaluate<ORDERED>(s, lut, code, steps, d0, odd, maxd);
+    r.expansions = 1;
+    for (;;) {
+        if (found >= 0) {
+            r.found_move = (uint16_t)td_tri_table[tri_base + T - 1 - found];
+            r.depth = level + 1;
+            r.status = TD_DFS_FOUND;
+            break;
         }
-        const int steps = (T + 31) >> 5;
-        const int tri_base = td_tri_base(N);
-        td_rate_masks(s, x);
-        if (lane == 0) {
-            s.L[0] = x.perm;
-            s.off[0] = x.offset;
+        if (r.expansions >= lim.max_expansions) {
+            r.status = TD_DFS_BUDGET;
+            break;
         }
-        __syncwarp();
-        int level = 0;
-        int odd = td_prepare_node(s, x.perm, x.offset, N);
-        int found = td_evaluate<ORDERED>(s, lut, code, steps, 0, odd, maxd);
-        expansions = 1;
-        for (;;) {
-            if (found >= 0) {
-                const uint32_t t = td_tri_table[tri_base + T - 1 - found];
-                found_move = (uint16_t)t;
-                depth = level + 1;
-                status = TD_FOUND;
-                break;
-            }
-            int accepted;
-            const int u = td_next_child<ORDERED>(s, level, &accepted);
-            if (u < 0) {
-                if (level == 0) break;  // exhausted: not found
-                --level;
-                continue;
-            }
-            const uint32_t t = td_tri_table[tri_base + T - 1 - u];
-            if (accepted) {
-                found_move = (uint16_t)t;
-                depth = level + 1;
-                status = TD_FOUND;
-                break;
-            }
-            if (expansions >= lim.max_expansions) {
-                status = TD_ERR_BUDGET;
-                break;
-            }
-            if ((expansions & 255u) == 0) {
-                int stop = 0;
-                if (lane == 0) {
-                    if (lim.deadline_ns && td_globaltimer() > lim.deadline_ns) stop = 1;
-                    if (lim.abort_flag && *(volatile const int *)lim.abort_flag) stop = 1;
-                }
-                if (__shfl_sync(TD_FULL, stop, 0)) {
-                    status = TD_ERR_TIMEOUT;
-                    break;
-                }
-            }
-            const int i = t & 31, j = (t >> 5) & 31, k = (t >> 10) & 31;
-            uint64_t nL;
-            int noff;
-            td_apply_move(s.L[level], s.off[level], N, i, j, k, &nL, &noff);
-            __syncwarp();
+        if (dc && (r.expansions % (uint32_t)dc->check_every) == 0) {
+            int hungry = 0, stop = 0;
             if (lane == 0) {
-                s.path[level] = (uint16_t)t;
-                s.L[level + 1] = nL;
-                s.off[level + 1] = (uint8_t)noff;
+                hungry = *(volatile int *)&dc->pool->idle;
+                stop = *(volatile int *)&dc->state->found;
             }
-            ++level;
-            odd = td_prepare_node(s, nL, noff, N);
-            found = td_evaluate<ORDERED>(s, lut, code, steps, level, odd, maxd);
-            ++expansions;
+            stop = __shfl_sync(TD_FULL, stop, 0);
+            if (stop) {
+                r.status = TD_DFS_ABORTED;
+                break;
+            }
+            hungry = __shfl_sync(TD_FULL, hungry, 0);
+            if (hungry > 0) td_donate(s, *dc, d0, level, N, T, tri_base, min(hungry, dc->grain));
         }
+        if ((r.expansions & 255u) == 0) {
+            int stop = 0;
+            if (lane == 0) {
+                if (lim.deadline_ns && td_globaltimer() > lim.deadline_ns) stop = 1;
+                if (lim.abort_flag && *(volatile const int *)lim.abort_flag) stop = 1;
+            }
+            if (__shfl_sync(TD_FULL, stop, 0)) {
+                r.status = TD_DFS_TIMEOUT;
+                break;
+            }
+        }
+        int accepted;
+        const int u = td_next_child<ORDERED>(s, level, &accepted);
+        if (u < 0) {
+            if (level == d0) break;  // this subtree is exhausted
+            --level;
+            continue;
+        }
+        const uint32_t t = td_tri_table[tri_base + T - 1 - u];
+        if (accepted) {
+            r.found_move = (uint16_t)t;
+            r.depth = level + 1;
+            r.status = TD_DFS_FOUND;
+            break;
+        }
+        uint64_t nL;
+        int noff;
+        td_apply_move(s.L[level], s.off[level], N, t & 31, (t >> 5) & 31, (t >> 10) & 31, &nL, &noff);
+        __syncwarp();
+        if (lane == 0) {
+            s.path[level] = (uint16_t)t;
+            s.L[level + 1] = nL;
+            s.off[level + 1] = (uint8_t)noff;
+        }
+        ++level;
+        odd = td_prepare_node(s, nL, noff, N);
+        found = td_evaluate<ORDERED>(s, lut, code, steps, level, odd, maxd);
+        ++r.expansions;
     }
     __syncwarp();
-    // write the 32-byte result: lanes 0..7 each store one word
+    return r;
+}
+
+__device__ __forceinline__ bool td_instance_ok(const td_instance &x) {
+    return x.n_symbols <= TD_MAX_N && x.max_moves >= 1 && x.max_moves <= TD_MAX_DEPTH &&
+           td_inst_init(x) <= TD_MAX_N;
+}
+
+// Loads codes for N and the instance's rate masks; places its root at level 0.
+__device__ __forceinline__ void td_setup_root(td_warp_smem &s, const td_instance &x, uint32_t (&code)[TD_MAX_STEPS],
+                                              int &codeN) {
+    const int lane = threadIdx.x & 31;
+    if (codeN != x.n_symbols) {
+        td_load_codes(x.n_symbols, code);
+        codeN = x.n_symbols;
+    }
+    td_rate_masks(s, x);
+    if (lane == 0) {
+        s.L[0] = x.perm;
+        s.off[0] = x.offset;
+    }
+    __syncwarp();
+}
+
+// Writes words [w0, w1) of a 32-byte result from lanes 0..7.
+__device__ __forceinline__ void td_write_result(td_result *out, int status, int depth, uint16_t found_move,
+                                                const uint16_t *path, uint32_t expansions, int w0, int w1) {
+    const int lane = threadIdx.x & 31;
     uint32_t word = 0;
     if (lane == 0) word = (uint32_t)status;
     else if (lane == 1) word = (uint32_t)depth;
@@ -339,12 +494,40 @@ __device__ void td_warp_search(const td_instance &x, td_result *out, td_warp_sme
         const int m0 = 2 * (lane - 2), m1 = m0 + 1;
         uint32_t lo = 0, hi = 0;
         if (status == TD_FOUND) {
-            if (m0 < depth) lo = (m0 == depth - 1) ? found_move : s.path[m0];
-            if (m1 < depth && m1 < TD_MAX_DEPTH) hi = (m1 == depth - 1) ? found_move : s.path[m1];
+            if (m0 < depth) lo = (m0 == depth - 1) ? found_move : path[m0];
+            if (m1 < depth && m1 < TD_MAX_DEPTH) hi = (m1 == depth - 1) ? found_move : path[m1];
         }
         word = lo | (hi << 16);
     } else if (lane == 7) {
         word = expansions;
     }
-    if (lane < 8) reinterpret_cast<uint32_t *>(out)[lane] = word;
+    if (lane >= w0 && lane < w1) reinterpret_cast<volatile uint32_t *>(out)[lane] = word;
+}
+
+// One complete search of instance x by the calling warp (no sharing).
+template <bool ORDERED>
+__device__ void td_warp_search(const td_instance &x, td_result *out, td_warp_smem &s,
+                               const uint8_t *lut, uint32_t (&code)[TD_MAX_STEPS], int &codeN,
+                               const td_search_limits &lim) {
+    int status = TD_NOT_FOUND, depth = 0;
+    uint32_t expansions = 0;
+    uint16_t found_move = 0;
+    if (!td_instance_ok(x)) {
+        status = TD_ERR_ARG;
+    } else if (td_triple_count(x.n_symbols) > 0) {
+        td_setup_root(s, x, code, codeN);
+        const td_dfs_out r = td_dfs<ORDERED>(s, lut, code, x.n_symbols, x.max_moves, 0, lim, nullptr);
+        expansions = r.expansions;
+        if (r.status == TD_DFS_FOUND) {
+            status = TD_FOUND;
+            depth = r.depth;
+            found_move = r.found_move;
+        } else if (r.status == TD_DFS_BUDGET) {
+            status = TD_ERR_BUDGET;
+        } else if (r.status == TD_DFS_TIMEOUT) {
+            status = TD_ERR_TIMEOUT;
+        }
+    }
+    __syncwarp();
+    td_write_result(out, status, depth, found_move, s.path, expansions, 0, 8);
 }

@@ -179,3 +179,29 @@ def test_edge_cases(slots):
     inst = td.prepare_perms(perms, n, 9)
     res, _ = td.search_batch(0, inst, ORDERED, max_expansions=2)
     assert (res["status"] == -2).any()
+
+
+def test_work_donation_keeps_verdicts_and_witnesses(slots, oracle):
+    """Hard n=13 instances at bound 7 (several exhaust their tree): with
+    donation forced at every expansion, verdicts equal the one-warp-per-
+    instance form and the oracle, and every witness replays."""
+    td = slots
+    perms, n = td.synth_perms(5, 2048, 13, 13, 100, 1, 3)
+    inst = td.prepare_perms(perms, n, 7)
+    td._lib.configure_steal(4, 6, 1)
+    try:
+        res, st = td.search_batch(0, inst, 0)
+        res2, st2 = td.search_batch(0, inst, 0)
+    finally:
+        td._lib.configure_steal(4, 4, 8)
+    assert st.donations > 0 and st.donated_items >= st.donations
+    plain, _ = td.search_batch(0, inst, PLAIN)
+    assert (res["status"] == plain["status"]).all() and (res2["status"] == plain["status"]).all()
+    assert st.errors == 0 and (res["status"] == 0).any()
+    beta, omega, init, N = _pairs(oracle, perms[:256], n[:256])
+    ost, _, _, _ = _oracle_batch(oracle, beta, omega, N, init, 0.0, 7, 1)
+    assert (res["status"][:256] == ost).all()
+    b2, o2, _, N2 = _pairs(oracle, perms, n)
+    _replay_all(oracle, b2, o2, N2, res, 7)
+    # expansions of a shared search are summed over every warp that took part
+    assert res["expansions"].sum() > 0
