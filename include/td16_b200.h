@@ -157,6 +157,15 @@ int td_search_batch_device(int slot, int count, const td_instance *d_instances,
                            uint64_t max_expansions, void *stream, char *err,
                            size_t errlen);
 
+/* CUDA-graph form of a batch over fixed device buffers: capture once, replay
+ * with one graph launch per batch (scratch epochs advance on the device). */
+int td_batch_graph_create(int slot, int count, const td_instance *d_instances,
+                          td_result *d_results, unsigned flags,
+                          uint64_t max_expansions, void **graph, char *err,
+                          size_t errlen);
+int td_batch_graph_launch(void *graph, void *stream, char *err, size_t errlen);
+int td_batch_graph_destroy(void *graph);
+
 /* Replays witnesses on the device with the reference checker's rules
  * (CertificateValidator.java:14-50): d_ok[i] = 1 when results[i] is a found
  * witness that sorts instance i within its max_moves, 0 otherwise. */
@@ -169,6 +178,65 @@ int td_validate_batch_device(int count, const td_instance *d_instances,
  * search kernel's roofline. */
 int td_int_issue_peak(int device, float target_ms, double *warp_inst_per_s,
                       double *ms, char *err, size_t errlen);
+
+/* ---- serving: continuous batching ---------------------------------------- */
+
+/* Starts a resident serving launch on `device`: requests published with
+ * td_serve_submit join the running launch as they arrive; each is searched
+ * by one warp with its DFS frames resident in shared memory.  The launch
+ * ends at td_serve_close (after draining) or after time_limit_s. */
+int td_serve_open(int device, unsigned ring_size, unsigned flags,
+                  double time_limit_s, void **handle, char *err, size_t errlen);
+int td_serve_workers(void *handle);
+/* TD_OVERFLOW while ring_size requests are unfinished */
+int td_serve_submit(void *handle, const td_instance *instance,
+                    unsigned long long *ticket);
+/* 1 (result copied) when done, else 0 */
+int td_serve_poll(void *handle, unsigned long long ticket, td_result *out);
+int td_serve_close(void *handle, char *err, size_t errlen);
+
+typedef struct td_serve_stats {
+    double p50_ms, p99_ms, p999_ms, mean_ms, max_ms;
+    double offered_per_s, served_per_s, wall_s;
+    double admission_wait_ms_mean;
+    uint64_t served, found;
+    int workers, max_inflight;
+} td_serve_stats;
+
+/* Open-loop Poisson experiment over `instances` at `rate` requests/s:
+ * admission when in-flight frame bytes (max_moves x frame) fit pool_bytes
+ * and a worker is free; latency from arrival to result on the host. */
+int td_serve_open_loop(int device, const td_instance *instances, int count,
+                       double rate, uint64_t seed, uint64_t pool_bytes,
+                       unsigned flags, td_result *results, td_serve_stats *stats,
+                       char *err, size_t errlen);
+
+/* ---- certificates (emitter/src/main/java/br/unb/cic/tdp/base/CertificateCodec.java) */
+
+/* key = omega one-line, 5 bits per symbol, MSB first (CertificateCodec.java:22-36);
+ * returns the byte length or -1 */
+int td_codec_key(const uint8_t *omega, int n, uint8_t *out, int cap);
+/* value = 15-bit (a,b,c) fields (CertificateCodec.java:56-72) */
+int td_codec_value(const uint8_t *abc, int count, uint8_t *out, int cap);
+/* decoders reject wrong lengths and nonzero padding (CertificateCodec.java:38-50,75-129) */
+int td_codec_decode_key(const uint8_t *in, int len, int n, uint8_t *omega);
+int td_codec_decode_value(const uint8_t *in, int len, uint8_t *abc, int cap_moves);
+
+/* Replays symbol witnesses on the device with CertificateValidator's rules
+ * (CertificateValidator.java:14-50).  Device pointers: beta/omega stride 17,
+ * n, max_moves, depth one byte each, abc stride 27. */
+int td_replay_symbols_device(int count, const uint8_t *d_beta, const uint8_t *d_omega,
+                             const uint8_t *d_n, const uint8_t *d_max_moves,
+                             const uint8_t *d_depth, const uint8_t *d_abc,
+                             uint8_t *d_ok, void *stream, char *err, size_t errlen);
+
+/* Batched certificate sink with AsyncCertificateWriter's queue-and-flush
+ * behaviour (AsyncCertificateWriter.java:50-116), writing flat records
+ * [key_len][value_len][key][value] (RocksDB is not part of this build). */
+void *td_cert_writer_open(const char *path, double flush_seconds);
+int td_cert_writer_enqueue(void *writer, const uint8_t *omega, int n,
+                           const uint8_t *abc, int count);
+long long td_cert_writer_close(void *writer);
 
 /* Position triples -> symbol triples on a copy of beta
  * (GPUSortingSearch.java:229-238). */

@@ -31,6 +31,16 @@ class BatchStats(C.Structure):
                 ("donations", C.c_uint64), ("donated_items", C.c_uint64)]
 
 
+class ServeStats(C.Structure):
+    _fields_ = [("p50_ms", C.c_double), ("p99_ms", C.c_double), ("p999_ms", C.c_double), ("mean_ms", C.c_double),
+                ("max_ms", C.c_double), ("offered_per_s", C.c_double), ("served_per_s", C.c_double),
+                ("wall_s", C.c_double), ("admission_wait_ms_mean", C.c_double), ("served", C.c_uint64),
+                ("found", C.c_uint64), ("workers", C.c_int), ("max_inflight", C.c_int)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class TdError(RuntimeError):
     def __init__(self, code: int, message: str):
         super().__init__(message)
@@ -42,7 +52,11 @@ _lib = None
 EXPORTS = ["td_init_slots", "td_search", "td_search_ordered", "td_slot_count", "td_slot_device",
            "td_slot_stream", "td_destroy", "td_prepare_pairs", "td_prepare_perms", "td_synth_perms",
            "td_search_batch", "td_search_batch_device", "td_validate_batch_device",
-           "td_positions_to_symbols", "td_configure", "td_configure_steal", "td_int_issue_peak"]
+           "td_positions_to_symbols", "td_configure", "td_configure_steal", "td_int_issue_peak",
+           "td_codec_key", "td_codec_value", "td_codec_decode_key", "td_codec_decode_value",
+           "td_replay_symbols_device", "td_cert_writer_open", "td_cert_writer_enqueue", "td_cert_writer_close",
+           "td_serve_open", "td_serve_workers", "td_serve_submit", "td_serve_poll", "td_serve_close",
+           "td_serve_open_loop", "td_batch_graph_create", "td_batch_graph_launch", "td_batch_graph_destroy"]
 
 
 def lib():
@@ -74,6 +88,26 @@ def lib():
     L.td_positions_to_symbols.restype = None
     L.td_configure.argtypes = [C.c_int, C.c_int]
     L.td_configure_steal.argtypes = [C.c_int, C.c_int, C.c_int]
+    L.td_codec_key.argtypes = [vp, C.c_int, vp, C.c_int]
+    L.td_codec_value.argtypes = [vp, C.c_int, vp, C.c_int]
+    L.td_codec_decode_key.argtypes = [vp, C.c_int, C.c_int, vp]
+    L.td_codec_decode_value.argtypes = [vp, C.c_int, vp, C.c_int]
+    L.td_replay_symbols_device.argtypes = [C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, cp, sz]
+    L.td_cert_writer_open.argtypes = [cp, C.c_double]
+    L.td_cert_writer_open.restype = vp
+    L.td_cert_writer_enqueue.argtypes = [vp, vp, C.c_int, vp, C.c_int]
+    L.td_cert_writer_close.argtypes = [vp]
+    L.td_cert_writer_close.restype = C.c_longlong
+    L.td_batch_graph_create.argtypes = [C.c_int, C.c_int, vp, vp, C.c_uint, C.c_uint64, C.POINTER(vp), cp, sz]
+    L.td_batch_graph_launch.argtypes = [vp, vp, cp, sz]
+    L.td_batch_graph_destroy.argtypes = [vp]
+    L.td_serve_open.argtypes = [C.c_int, C.c_uint, C.c_uint, C.c_double, C.POINTER(vp), cp, sz]
+    L.td_serve_workers.argtypes = [vp]
+    L.td_serve_submit.argtypes = [vp, vp, C.POINTER(C.c_ulonglong)]
+    L.td_serve_poll.argtypes = [vp, C.c_ulonglong, vp]
+    L.td_serve_close.argtypes = [vp, cp, sz]
+    L.td_serve_open_loop.argtypes = [C.c_int, vp, C.c_int, C.c_double, C.c_uint64, C.c_uint64, C.c_uint, vp,
+                                     C.POINTER(ServeStats), cp, sz]
     _lib = L
     return L
 
@@ -208,3 +242,141 @@ def configure_steal(grain: int, split_level: int, check_every: int) -> None:
 
 def unpack_moves(row) -> list:
     return [(int(m) & 31, (int(m) >> 5) & 31, (int(m) >> 10) & 31) for m in row["moves"][: int(row["depth"])]]
+
+
+# ---- certificate format (CertificateCodec.java) ----------------------------
+
+def codec_key(omega) -> bytes:
+    o = np.frombuffer(bytes(omega), np.uint8).copy()
+    out = np.zeros(32, np.uint8)
+    n = lib().td_codec_key(_ptr(o), len(o), _ptr(out), 32)
+    if n < 0:
+        raise TdError(INVALID_ARG, "certificate keys need 1..32 symbols below 32")
+    return out[:n].tobytes()
+
+
+def codec_value(abc_moves) -> bytes:
+    flat = np.asarray([v for m in abc_moves for v in m] or [0], np.uint8)
+    out = np.zeros(64, np.uint8)
+    n = lib().td_codec_value(_ptr(flat), len(abc_moves), _ptr(out), 64)
+    if n < 0:
+        raise TdError(INVALID_ARG, "a certificate must contain at least one move of symbols below 32")
+    return out[:n].tobytes()
+
+
+def codec_decode_key(data: bytes, n: int):
+    d = np.frombuffer(bytes(data) or b"\0", np.uint8).copy()
+    out = np.zeros(32, np.uint8)
+    if lib().td_codec_decode_key(_ptr(d), len(data), int(n), _ptr(out)) < 0:
+        raise TdError(INVALID_ARG, "malformed certificate key")
+    return out[:n].tolist()
+
+
+def codec_decode_value(data: bytes):
+    d = np.frombuffer(bytes(data) or b"\0", np.uint8).copy()
+    out = np.zeros(96, np.uint8)
+    k = lib().td_codec_decode_value(_ptr(d), len(data), _ptr(out), 32)
+    if k < 0:
+        raise TdError(INVALID_ARG, "malformed certificate value")
+    return [tuple(int(v) for v in out[3 * m: 3 * m + 3]) for m in range(k)]
+
+
+class CertificateWriter:
+    """Batched flat-file sink of certificate records (AsyncCertificateWriter semantics)."""
+
+    def __init__(self, path: str, flush_seconds: float = 5.0):
+        self._h = lib().td_cert_writer_open(path.encode(), float(flush_seconds))
+        if not self._h:
+            raise TdError(INVALID_ARG, f"cannot open {path}")
+
+    def enqueue(self, omega, abc_moves) -> None:
+        o = np.frombuffer(bytes(omega), np.uint8).copy()
+        flat = np.asarray([v for m in abc_moves for v in m] or [0], np.uint8)
+        rc = lib().td_cert_writer_enqueue(self._h, _ptr(o), len(o), _ptr(flat), len(abc_moves))
+        if rc == -2:
+            raise TdError(CUDA_ERROR, "certificate writer failed")
+        if rc != 0:
+            raise TdError(INVALID_ARG, "unencodable certificate")
+
+    def close(self) -> int:
+        n = lib().td_cert_writer_close(self._h)
+        self._h = None
+        if n < 0:
+            raise TdError(CUDA_ERROR, "certificate writer failed")
+        return int(n)
+
+
+def read_certificates(path: str):
+    """Reads the flat file written by CertificateWriter: [(key, value), ...]."""
+    data = open(path, "rb").read()
+    out, i = [], 0
+    while i < len(data):
+        kl, vl = data[i], data[i + 1]
+        out.append((data[i + 2: i + 2 + kl], data[i + 2 + kl: i + 2 + kl + vl]))
+        i += 2 + kl + vl
+    return out
+
+
+# ---- serving (continuous batching) -----------------------------------------
+
+class Server:
+    """A resident serving launch: submit requests while others run."""
+
+    def __init__(self, device: int = 0, ring_size: int = 4096, flags: int = 0, time_limit_s: float = 60.0):
+        h = C.c_void_p()
+        err = C.create_string_buffer(512)
+        check(lib().td_serve_open(int(device), int(ring_size), int(flags), float(time_limit_s), C.byref(h), err, 512),
+              err)
+        self._h = h
+        self.workers = lib().td_serve_workers(h)
+
+    def submit(self, instance) -> int:
+        x = np.ascontiguousarray(np.asarray(instance, INSTANCE_DTYPE).reshape(1))
+        t = C.c_ulonglong()
+        rc = lib().td_serve_submit(self._h, _ptr(x), C.byref(t))
+        if rc != OK:
+            raise TdError(rc, "serving ring is full")
+        return t.value
+
+    def poll(self, ticket: int):
+        out = np.zeros(1, RESULT_DTYPE)
+        return out[0] if lib().td_serve_poll(self._h, C.c_ulonglong(ticket), _ptr(out)) else None
+
+    def close(self) -> None:
+        err = C.create_string_buffer(512)
+        check(lib().td_serve_close(self._h, err, 512), err)
+        self._h = None
+
+
+def serve_open_loop(device: int, instances: np.ndarray, rate: float, seed: int = 3,
+                    pool_bytes: int = 64 << 30, flags: int = 0):
+    """Open-loop Poisson experiment; returns (results, stats dict)."""
+    instances = np.ascontiguousarray(instances, INSTANCE_DTYPE)
+    results = np.zeros(len(instances), RESULT_DTYPE)
+    st = ServeStats()
+    err = C.create_string_buffer(512)
+    rc = lib().td_serve_open_loop(int(device), _ptr(instances), len(instances), float(rate), C.c_uint64(seed),
+                                  C.c_uint64(pool_bytes), int(flags), _ptr(results), C.byref(st), err, 512)
+    check(rc, err)
+    return results, st.as_dict()
+
+
+class BatchGraph:
+    """A captured batch launch over fixed device buffers (CUDA graph)."""
+
+    def __init__(self, slot: int, count: int, d_instances: int, d_results: int, flags: int = 0,
+                 max_expansions: int = 0):
+        h = C.c_void_p()
+        err = C.create_string_buffer(512)
+        check(lib().td_batch_graph_create(int(slot), int(count), C.c_void_p(d_instances), C.c_void_p(d_results),
+                                          int(flags), C.c_uint64(max_expansions), C.byref(h), err, 512), err)
+        self._h = h
+
+    def launch(self, stream: int | None = None) -> None:
+        err = C.create_string_buffer(512)
+        check(lib().td_batch_graph_launch(self._h, C.c_void_p(stream) if stream else None, err, 512), err)
+
+    def close(self) -> None:
+        if self._h:
+            lib().td_batch_graph_destroy(self._h)
+            self._h = None

@@ -26,7 +26,7 @@ def nvcc() -> str:
 
 
 def _sources():
-    return [os.path.join(CSRC, "td_engine.cu")]
+    return [os.path.join(CSRC, "td_engine.cu"), os.path.join(CSRC, "td_cert.cu")]
 
 
 def _deps():

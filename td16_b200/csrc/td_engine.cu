@@ -12,7 +12,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <cmath>
+#include <thread>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -152,7 +155,7 @@ __device__ __forceinline__ void td_finish_unit(const td_dfs_out &r, td_inst_stat
 
 __global__ void __launch_bounds__(256) td_steal_kernel(const td_instance *__restrict__ in,
                                                       td_result *__restrict__ out, int count, td_pool *pool,
-                                                      td_item *items, uint32_t *ready, uint32_t epoch,
+                                                      td_item *items, uint32_t *ready, const uint32_t *epoch_ptr,
                                                       int capacity, td_inst_state *state, int grain,
                                                       int max_level, int check_every, uint64_t time_limit_ns) {
     extern __shared__ __align__(16) uint8_t td_smem[];
@@ -168,6 +171,7 @@ __global__ void __launch_bounds__(256) td_steal_kernel(const td_instance *__rest
     dc.pool = pool;
     dc.items = items;
     dc.ready = ready;
+    const uint32_t epoch = *epoch_ptr;  // bumped by td_epoch_kernel before this launch
     dc.epoch = epoch;
     dc.capacity = capacity;
     dc.grain = grain;
@@ -284,6 +288,14 @@ __global__ void __launch_bounds__(256) td_steal_kernel(const td_instance *__rest
     if (lane == 0 && idle) atomicSub(&pool->idle, 1);
 }
 
+// Advances the launch epoch that tags donated items as written; a launch
+// replayed from a CUDA graph therefore never mistakes an item of an earlier
+// launch for one of its own.
+__global__ void td_epoch_kernel(uint32_t *epoch) {
+    uint32_t e = *epoch + 1;
+    *epoch = e ? e : 1;
+}
+
 // Witness replay in pinned form: every move must be an in-range position
 // triple i<j<k, at most max_moves of them, and the final state must be the
 // identity (omega = id  <=>  beta = rho  <=>  L = 0,1,...,n-1).
@@ -360,7 +372,7 @@ struct Slot {
     int item_capacity = 0;
     td_inst_state *d_state = nullptr;
     size_t state_count = 0;
-    uint32_t epoch = 0;
+    uint32_t *d_epoch = nullptr;
     std::mutex *mu = nullptr;
 };
 
@@ -448,6 +460,7 @@ void release_slot(Slot &s) {
     if (s.d_pool) cudaFree(s.d_pool);
     if (s.d_items) cudaFree(s.d_items);
     if (s.d_ready) cudaFree(s.d_ready);
+    if (s.d_epoch) cudaFree(s.d_epoch);
     if (s.d_state) cudaFree(s.d_state);
     if (s.h_inst) cudaFreeHost(s.h_inst);
     if (s.h_res) cudaFreeHost(s.h_res);
@@ -485,6 +498,8 @@ int launch_batch(Slot &s, int count, const td_instance *d_in, td_result *d_out, 
             TD_CHECK(cudaMalloc(&s.d_items, cap * sizeof(td_item)));
             TD_CHECK(cudaMalloc(&s.d_ready, cap * sizeof(uint32_t)));
             TD_CHECK(cudaMemset(s.d_ready, 0, cap * sizeof(uint32_t)));
+            TD_CHECK(cudaMalloc(&s.d_epoch, sizeof(uint32_t)));
+            TD_CHECK(cudaMemset(s.d_epoch, 0, sizeof(uint32_t)));
             s.item_capacity = (int)cap;
         }
         if ((size_t)count > s.state_count) {
@@ -493,10 +508,6 @@ int launch_batch(Slot &s, int count, const td_instance *d_in, td_result *d_out, 
             s.state_count = 0;
             TD_CHECK(cudaMalloc(&s.d_state, (size_t)count * sizeof(td_inst_state)));
             s.state_count = (size_t)count;
-        }
-        if (++s.epoch == 0) {  // ready flags from 2^32 launches ago could alias
-            TD_CHECK(cudaMemsetAsync(s.d_ready, 0, (size_t)s.item_capacity * sizeof(uint32_t), stream));
-            s.epoch = 1;
         }
         DeviceInfo &d = g_dev[s.device];
         if (d.steal_blocks_per_sm == 0) {
@@ -507,7 +518,8 @@ int launch_batch(Slot &s, int count, const td_instance *d_in, td_result *d_out, 
         const int grid = std::max(1, std::min(d.sms * d.steal_blocks_per_sm, (count + warps - 1) / warps));
         TD_CHECK(cudaMemsetAsync(s.d_pool, 0, sizeof(td_pool), stream));
         TD_CHECK(cudaMemsetAsync(s.d_state, 0, (size_t)count * sizeof(td_inst_state), stream));
-        td_steal_kernel<<<grid, threads, smem, stream>>>(d_in, d_out, count, s.d_pool, s.d_items, s.d_ready, s.epoch,
+        td_epoch_kernel<<<1, 1, 0, stream>>>(s.d_epoch);
+        td_steal_kernel<<<grid, threads, smem, stream>>>(d_in, d_out, count, s.d_pool, s.d_items, s.d_ready, s.d_epoch,
                                                          s.item_capacity, s.d_state, g_steal_grain, g_split_level,
                                                          g_check_every, time_limit_ns());
     } else {
@@ -995,3 +1007,77 @@ TD_API int td_int_issue_peak(int device, float target_ms, double *warp_inst_per_
     if (ms_out) *ms_out = ms;
     return TD_OK;
 }
+
+// ---- CUDA graphs -------------------------------------------------------------
+
+namespace {
+struct BatchGraph {
+    int device;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+}  // namespace
+
+// Captures one batch launch (search, and the device replay when flags has
+// TD_FLAG_VERIFY) over fixed device buffers into a CUDA graph.  Replaying it
+// with td_batch_graph_launch costs one graph launch per batch.
+TD_API int td_batch_graph_create(int slot, int count, const td_instance *d_in, td_result *d_out, unsigned flags,
+                                 uint64_t max_exp, void **out_graph, char *err, size_t errlen) {
+    Slot *s;
+    {
+        std::lock_guard<std::mutex> g(g_mu);
+        s = get_slot(slot, err, errlen);
+        if (!s) return TD_INVALID_ARG;
+    }
+    if (!out_graph || count <= 0) {
+        set_err(err, errlen, "invalid graph arguments");
+        return TD_INVALID_ARG;
+    }
+    std::lock_guard<std::mutex> g(*s->mu);
+    TD_CHECK(cudaSetDevice(s->device));
+    // one eager launch sizes the slot's scratch outside the capture
+    int rc = launch_batch(*s, count, d_in, d_out, flags, max_exp, s->stream, err, errlen);
+    if (rc != TD_OK) return rc;
+    TD_CHECK(cudaStreamSynchronize(s->stream));
+    auto *bg = new BatchGraph();
+    bg->device = s->device;
+    cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        rc = launch_batch(*s, count, d_in, d_out, flags, max_exp, s->stream, err, errlen);
+        e = cudaStreamEndCapture(s->stream, &bg->graph);
+        if (rc != TD_OK) {
+            if (bg->graph) cudaGraphDestroy(bg->graph);
+            delete bg;
+            return rc;
+        }
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&bg->exec, bg->graph, 0);
+    if (e != cudaSuccess) {
+        if (bg->graph) cudaGraphDestroy(bg->graph);
+        delete bg;
+        set_err(err, errlen, cuda_msg(e, __FILE__, __LINE__));
+        return TD_CUDA_ERROR;
+    }
+    *out_graph = bg;
+    return TD_OK;
+}
+
+TD_API int td_batch_graph_launch(void *graph, void *stream, char *err, size_t errlen) {
+    auto *bg = static_cast<BatchGraph *>(graph);
+    if (!bg) return TD_INVALID_ARG;
+    TD_CHECK(cudaSetDevice(bg->device));
+    TD_CHECK(cudaGraphLaunch(bg->exec, (cudaStream_t)stream));
+    return TD_OK;
+}
+
+TD_API int td_batch_graph_destroy(void *graph) {
+    auto *bg = static_cast<BatchGraph *>(graph);
+    if (!bg) return TD_INVALID_ARG;
+    cudaSetDevice(bg->device);
+    if (bg->exec) cudaGraphExecDestroy(bg->exec);
+    if (bg->graph) cudaGraphDestroy(bg->graph);
+    delete bg;
+    return TD_OK;
+}
+
+#include "td_serve.cuh"

@@ -30,6 +30,7 @@ struct td_warp_smem {
     uint32_t reach[TD_MAX_DEPTH + 2];          // prune mask over odd counts, per depth
     uint16_t path[TD_MAX_DEPTH];               // caller-position move per level
     uint8_t off[TD_MAX_DEPTH + 1];
+    alignas(16) uint16_t md[24];               // cycle descriptor by caller position
 };
 
 // Lexicographic position triples i|j<<5|k<<10 for every N, at offset C(N,4).
@@ -78,54 +79,68 @@ __device__ __forceinline__ int td_prepare_node(td_warp_smem &s, uint64_t L, int 
     uint32_t y = Bq + 1;
     if (y == (uint32_t)N) y = 0;
     const int nx = act ? (y ? (int)td_nib(inv, (int)y - 1) + 1 : 0) : p;
-    // leader = smallest position on the cycle
-    int m = p, j = nx;
+    // leader = smallest position on the cycle and dist = omega steps to it,
+    // in one pointer-jumping pass: each lane keeps the minimum of the window
+    // p, next(p), ..., next^(w-1)(p) and its distance; windows double per round
+    // and 32 >= any cycle length, so the first occurrence of the minimum wins.
+    int m = p, d = 0, j = nx;
 #pragma unroll
     for (int r = 0; r < 5; ++r) {
-        const int mm = __shfl_sync(TD_FULL, m, j);
-        m = min(m, mm);
-        j = __shfl_sync(TD_FULL, j, j);
+        const int mB = __shfl_sync(TD_FULL, m, j);
+        const int dB = __shfl_sync(TD_FULL, d, j);
+        const int jB = __shfl_sync(TD_FULL, j, j);
+        if (mB < m) {
+            m = mB;
+            d = (1 << r) + dB;
+        }
+        j = jB;
     }
     const bool leader = m == p;
-    // dist = omega steps to the leader (list ranking with the cycle cut there)
-    int d = leader ? 0 : 1;
-    j = leader ? p : nx;
-#pragma unroll
-    for (int r = 0; r < 5; ++r) {
-        d += __shfl_sync(TD_FULL, d, j);
-        j = __shfl_sync(TD_FULL, j, j);
-    }
     const int after_leader = __shfl_sync(TD_FULL, nx, m);
     const int len = __shfl_sync(TD_FULL, d, after_leader) + 1;
     const int odd = __popc(__ballot_sync(TD_FULL, act && leader && (len & 1)));
-    // pair table row of this lane's caller position
-    const uint32_t md = (uint32_t)m | ((uint32_t)d << 8);
-    const uint32_t o3 = (uint32_t)(len & 1) << 3;
-    const uint32_t fixed4 = len == 1 ? 4u : 0u;
+    // descriptors by caller position: md = leader | dist << 5
     int rp = p - off;
     rp += rp < 0 ? N : 0;
-    uint8_t *row = &s.pt[rp * TD_PT_STRIDE];
-    int q = off;  // pinned position of caller position 0
-    uint32_t word = 0;
-    for (int rq = 0; rq < N; ++rq) {
-        const uint32_t mdq = __shfl_sync(TD_FULL, md, q);
-        const uint32_t x = md ^ mdq;
+    const uint32_t md = (uint32_t)m | ((uint32_t)d << 5);
+    if (act) s.md[rp] = (uint16_t)md;
+    __syncwarp();
+    uint16_t mdq[24];
+    {
+        const uint4 *src = reinterpret_cast<const uint4 *>(s.md);
+        uint4 v0 = src[0], v1 = src[1], v2 = src[2];
+        const uint32_t w[12] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w, v2.x, v2.y, v2.z, v2.w};
+#pragma unroll
+        for (int k = 0; k < 12; ++k) {
+            mdq[2 * k] = (uint16_t)(w[k] & 0xffffu);
+            mdq[2 * k + 1] = (uint16_t)(w[k] >> 16);
+        }
+    }
+    // pair table row of this lane's caller position
+    const uint32_t o3 = (uint32_t)(len & 1) << 3;
+    const uint32_t fixed4 = len == 1 ? 4u : 0u;
+    uint32_t row[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) row[k] = 0;
+#pragma unroll
+    for (int rq = 0; rq < TD_MAX_N; ++rq) {
+        const uint32_t q = mdq[rq];
+        const uint32_t x = md ^ q;
         uint32_t e;
-        if ((x & 0xffu) == 0) {
-            const uint32_t g = md > mdq ? 1u : 0u;  // same leader: compares dist
-            uint32_t w = (x >> 8) & 1u;              // parity of dist difference
-            w ^= (o3 >> 3) & (g ^ 1u);               // wrap of an odd cycle flips it
+        if ((x & 31u) == 0) {
+            const uint32_t g = md > q ? 1u : 0u;   // same leader: compares dist
+            uint32_t w = (x >> 5) & 1u;            // parity of the dist difference
+            w ^= (o3 >> 3) & (g ^ 1u);             // wrap of an odd cycle flips it
             e = 1u | (w << 1) | (g << 2) | o3;
         } else {
             e = fixed4 | o3;
         }
-        word |= e << (8 * (rq & 3));
-        if ((rq & 3) == 3 || rq == N - 1) {
-            if (act) *reinterpret_cast<uint32_t *>(row + (rq & ~3)) = word;
-            word = 0;
-        }
-        ++q;
-        q -= q >= N ? N : 0;
+        row[rq >> 2] |= e << (8 * (rq & 3));
+    }
+    if (act) {
+        uint32_t *dst = reinterpret_cast<uint32_t *>(&s.pt[rp * TD_PT_STRIDE]);
+        *reinterpret_cast<uint4 *>(dst) = make_uint4(row[0], row[1], row[2], row[3]);
+        dst[4] = row[4];
     }
     return odd;
 }

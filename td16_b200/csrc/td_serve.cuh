@@ -1,0 +1,407 @@
+// td_serve.cuh -- continuous-batching serving loop (included by td_engine.cu).
+//
+// A resident kernel serves search requests as they arrive.  The host publishes
+// request r into slot r % R of a pinned, device-mapped ring and advances
+// `published`; one dispatcher warp polls that counter (one PCIe read per
+// poll), copies new requests into a device queue and raises `available`.
+// Worker warps claim requests in arrival order, run the search with their DFS
+// frames resident in shared memory, write the result into the mapped result
+// ring and stamp done[r % R] = r + 1.  Requests that arrive while others run
+// join the same launch: there is no batch boundary.  Every wait is bounded by
+// the launch deadline; the launch ends when the host raises `stop` and every
+// published request has been served.
+#pragma once
+
+struct td_serve_host_ctl {     // pinned, mapped: written by the host
+    volatile unsigned long long published;
+    volatile int stop;
+    int pad;
+};
+
+struct td_serve_dev_ctl {      // device memory: scheduler state of the launch
+    unsigned long long available;
+    unsigned long long claimed;
+    int stop;
+    int error;
+    unsigned long long served;
+};
+
+template <bool ORDERED>
+__global__ void __launch_bounds__(256) td_serve_kernel(const td_instance *ring, td_result *results,
+                                                      volatile unsigned long long *done, unsigned ring_size,
+                                                      td_serve_host_ctl *hctl, td_serve_dev_ctl *dctl,
+                                                      td_instance *queue, uint64_t max_exp,
+                                                      uint64_t time_limit_ns) {
+    extern __shared__ __align__(16) uint8_t td_smem[];
+    const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint8_t *lut = td_smem;
+    td_warp_smem *ws = reinterpret_cast<td_warp_smem *>(td_smem + TD_LUT_BYTES);
+    td_block_init(lut, ws, warps);
+    const uint64_t deadline = td_globaltimer() + time_limit_ns;
+    if (blockIdx.x == 0 && warp == 0) {
+        // dispatcher: host ring -> device queue
+        unsigned long long avail = 0;
+        unsigned backoff = 256;
+        for (;;) {
+            const int hstop = hctl->stop;
+            const unsigned long long pub = hctl->published;  // read after stop: a stop is never ahead of its requests
+            if (pub > avail) {
+                for (unsigned long long r = avail + lane; r < pub; r += 32) {
+                    const uint4 v = __ldcv(reinterpret_cast<const uint4 *>(&ring[r % ring_size]));
+                    *reinterpret_cast<uint4 *>(&queue[r % ring_size]) = v;
+                }
+                __threadfence();
+                __syncwarp();
+                if (lane == 0) atomicExch(&dctl->available, pub);
+                avail = pub;
+                backoff = 256;
+                continue;
+            }
+            if (hstop) {
+                if (lane == 0) atomicExch(&dctl->stop, 1);
+                break;
+            }
+            if (td_globaltimer() > deadline) {
+                if (lane == 0) {
+                    atomicCAS(&dctl->error, 0, TD_ERR_TIMEOUT);
+                    atomicExch(&dctl->stop, 1);
+                }
+                break;
+            }
+            __nanosleep(backoff);
+            backoff = min(backoff * 2u, 2048u);
+        }
+        return;
+    }
+    td_warp_smem &s = ws[warp];
+    uint32_t code[TD_MAX_STEPS];
+    int codeN = -1;
+    td_search_limits lim;
+    lim.max_expansions = max_exp ? max_exp : ~0ull;
+    lim.deadline_ns = deadline;
+    lim.abort_flag = nullptr;
+    unsigned backoff = 128;
+    for (;;) {
+        long long r = -1;
+        int stop = 0;
+        if (lane == 0) {
+            const unsigned long long av = *(volatile unsigned long long *)&dctl->available;
+            unsigned long long c = *(volatile unsigned long long *)&dctl->claimed;
+            while (c < av) {
+                const unsigned long long prev = atomicCAS(&dctl->claimed, c, c + 1);
+                if (prev == c) { r = (long long)c; break; }
+                c = prev;
+            }
+            if (r < 0) {
+                stop = *(volatile int *)&dctl->stop;
+                if (stop) {  // drain: the dispatcher publishes before it stops
+                    const unsigned long long av2 = *(volatile unsigned long long *)&dctl->available;
+                    const unsigned long long c2 = *(volatile unsigned long long *)&dctl->claimed;
+                    stop = c2 >= av2;
+                }
+                if (td_globaltimer() > deadline) stop = 1;
+            }
+            __threadfence();
+        }
+        r = __shfl_sync(TD_FULL, r, 0);
+        if (r < 0) {
+            if (__shfl_sync(TD_FULL, stop, 0)) break;
+            __nanosleep(backoff);
+            backoff = min(backoff * 2u, 1024u);
+            continue;
+        }
+        backoff = 128;
+        const unsigned slot = (unsigned)(r % ring_size);
+        td_instance x;
+        {
+            const uint4 v = __ldcg(reinterpret_cast<const uint4 *>(&queue[slot]));
+            x = *reinterpret_cast<const td_instance *>(&v);
+        }
+        td_result *res = &results[slot];
+        td_warp_search<ORDERED>(x, res, s, lut, code, codeN, lim);
+        __threadfence_system();
+        __syncwarp();
+        if (lane == 0) {
+            done[slot] = (unsigned long long)r + 1ull;
+            atomicAdd(&dctl->served, 1ull);
+        }
+    }
+}
+
+// ============================================================================
+// host side of the serving loop
+// ============================================================================
+
+namespace {
+
+struct Server {
+    int device = -1;
+    unsigned flags = 0;
+    cudaStream_t stream = nullptr;
+    unsigned R = 0;
+    td_instance *h_ring = nullptr, *d_ring = nullptr;
+    td_result *h_res = nullptr, *d_res = nullptr;
+    unsigned long long *h_done = nullptr, *d_done = nullptr;
+    td_serve_host_ctl *h_ctl = nullptr, *d_hctl = nullptr;
+    td_serve_dev_ctl *d_ctl = nullptr;
+    td_instance *d_queue = nullptr;
+    unsigned long long published = 0;
+    int workers = 0;
+};
+
+void server_free(Server *sv) {
+    if (!sv) return;
+    if (sv->device >= 0) cudaSetDevice(sv->device);
+    if (sv->stream) cudaStreamSynchronize(sv->stream);
+    if (sv->h_ring) cudaFreeHost(sv->h_ring);
+    if (sv->h_res) cudaFreeHost(sv->h_res);
+    if (sv->h_done) cudaFreeHost(sv->h_done);
+    if (sv->h_ctl) cudaFreeHost(sv->h_ctl);
+    if (sv->d_ctl) cudaFree(sv->d_ctl);
+    if (sv->d_queue) cudaFree(sv->d_queue);
+    if (sv->stream) cudaStreamDestroy(sv->stream);
+    delete sv;
+}
+
+}  // namespace
+
+// Starts a resident serving launch on `device` with a ring of `ring_size`
+// requests.  flags: TD_FLAG_ORDERED for the reference order.  The launch ends
+// after td_serve_close or after time_limit_s.
+TD_API int td_serve_open(int device, unsigned ring_size, unsigned flags, double time_limit_s, void **handle,
+                         char *err, size_t errlen) {
+    if (!handle || ring_size < 2 || ring_size > (1u << 24)) {
+        set_err(err, errlen, "invalid serving arguments");
+        return TD_INVALID_ARG;
+    }
+    {
+        std::lock_guard<std::mutex> g(g_mu);
+        const int rc = ensure_device(device, err, errlen);
+        if (rc != TD_OK) return rc;
+    }
+    auto *sv = new Server();
+    sv->device = device;
+    sv->flags = flags;
+    sv->R = ring_size;
+    auto fail = [&](cudaError_t e, int line) {
+        set_err(err, errlen, cuda_msg(e, __FILE__, line));
+        server_free(sv);
+        return TD_CUDA_ERROR;
+    };
+    cudaError_t e;
+    if ((e = cudaSetDevice(device)) != cudaSuccess) return fail(e, __LINE__);
+    if ((e = cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, __LINE__);
+    const unsigned mapped = cudaHostAllocMapped | cudaHostAllocPortable;
+    if ((e = cudaHostAlloc(&sv->h_ring, sizeof(td_instance) * ring_size, mapped)) != cudaSuccess) return fail(e, __LINE__);
+    if ((e = cudaHostAlloc(&sv->h_res, sizeof(td_result) * ring_size, mapped)) != cudaSuccess) return fail(e, __LINE__);
+    if ((e = cudaHostAlloc(&sv->h_done, sizeof(unsigned long long) * ring_size, mapped)) != cudaSuccess) return fail(e, __LINE__);
+    if ((e = cudaHostAlloc(&sv->h_ctl, sizeof(td_serve_host_ctl), mapped)) != cudaSuccess) return fail(e, __LINE__);
+    std::memset((void *)sv->h_done, 0, sizeof(unsigned long long) * ring_size);
+    std::memset((void *)sv->h_ctl, 0, sizeof(td_serve_host_ctl));
+    if ((e = cudaHostGetDevicePointer(&sv->d_ring, sv->h_ring, 0)) != cudaSuccess) return fail(e, __LINE__);
+    if ((e = cudaHostGetDevicePointer(&sv->d_res, sv->h_res, 0)) != cudaSuccess) return fail(e, __LINE__);
+    if ((e = cudaHostGetDevicePointer(&sv->d_done, sv->h_done, 0)) != cudaSuccess) return fail(e, __LINE__);
+    if ((e = cudaHostGetDevicePointer(&sv->d_hctl, sv->h_ctl, 0)) != cudaSuccess) return fail(e, __LINE__);
+    if ((e = cudaMalloc(&sv->d_ctl, sizeof(td_serve_dev_ctl))) != cudaSuccess) return fail(e, __LINE__);
+    if ((e = cudaMalloc(&sv->d_queue, sizeof(td_instance) * ring_size)) != cudaSuccess) return fail(e, __LINE__);
+    if ((e = cudaMemsetAsync(sv->d_ctl, 0, sizeof(td_serve_dev_ctl), sv->stream)) != cudaSuccess) return fail(e, __LINE__);
+    const int warps = g_warps_per_block;
+    const size_t smem = smem_bytes(warps);
+    int per_sm = 0;
+    const bool ordered = flags & TD_FLAG_ORDERED;
+    if (ordered) {
+        if ((e = cudaFuncSetAttribute(td_serve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) return fail(e, __LINE__);
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, td_serve_kernel<true>, warps * 32, smem)) != cudaSuccess) return fail(e, __LINE__);
+    } else {
+        if ((e = cudaFuncSetAttribute(td_serve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) return fail(e, __LINE__);
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, td_serve_kernel<false>, warps * 32, smem)) != cudaSuccess) return fail(e, __LINE__);
+    }
+    const int grid = g_dev[device].sms * std::max(1, per_sm);
+    sv->workers = grid * warps - 1;
+    const uint64_t limit_ns = (uint64_t)((time_limit_s > 0 ? time_limit_s : 60.0) * 1e9);
+    if (ordered)
+        td_serve_kernel<true><<<grid, warps * 32, smem, sv->stream>>>(sv->d_ring, sv->d_res, sv->d_done, ring_size,
+                                                                      sv->d_hctl, sv->d_ctl, sv->d_queue, 0, limit_ns);
+    else
+        td_serve_kernel<false><<<grid, warps * 32, smem, sv->stream>>>(sv->d_ring, sv->d_res, sv->d_done, ring_size,
+                                                                       sv->d_hctl, sv->d_ctl, sv->d_queue, 0, limit_ns);
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, __LINE__);
+    *handle = sv;
+    return TD_OK;
+}
+
+TD_API int td_serve_workers(void *handle) { return handle ? static_cast<Server *>(handle)->workers : 0; }
+
+// Publishes one request; *ticket receives its sequence number.  Returns
+// TD_OVERFLOW when the ring still holds ring_size unfinished requests.
+TD_API int td_serve_submit(void *handle, const td_instance *x, unsigned long long *ticket) {
+    auto *sv = static_cast<Server *>(handle);
+    const unsigned long long r = sv->published;
+    const unsigned slot = (unsigned)(r % sv->R);
+    if (r >= sv->R && __atomic_load_n(&sv->h_done[slot], __ATOMIC_ACQUIRE) != r - sv->R + 1) return TD_OVERFLOW;
+    sv->h_ring[slot] = *x;
+    __atomic_store_n(&sv->h_done[slot], 0ull, __ATOMIC_RELAXED);
+    __atomic_thread_fence(__ATOMIC_SEQ_CST);
+    sv->published = r + 1;
+    __atomic_store_n(const_cast<unsigned long long *>(&sv->h_ctl->published), r + 1, __ATOMIC_RELEASE);
+    if (ticket) *ticket = r;
+    return TD_OK;
+}
+
+// 1 and the result when request `ticket` is done, 0 while it runs.
+TD_API int td_serve_poll(void *handle, unsigned long long ticket, td_result *out) {
+    auto *sv = static_cast<Server *>(handle);
+    const unsigned slot = (unsigned)(ticket % sv->R);
+    if (__atomic_load_n(&sv->h_done[slot], __ATOMIC_ACQUIRE) != ticket + 1) return 0;
+    if (out) std::memcpy(out, (const void *)&sv->h_res[slot], sizeof(td_result));
+    return 1;
+}
+
+// Stops the launch after every published request is served; returns
+// TD_TIMEOUT if the launch hit its deadline.
+TD_API int td_serve_close(void *handle, char *err, size_t errlen) {
+    auto *sv = static_cast<Server *>(handle);
+    if (!sv) return TD_INVALID_ARG;
+    __atomic_store_n(const_cast<int *>(&sv->h_ctl->stop), 1, __ATOMIC_RELEASE);
+    cudaSetDevice(sv->device);
+    cudaError_t e = cudaStreamSynchronize(sv->stream);
+    td_serve_dev_ctl ctl;
+    std::memset(&ctl, 0, sizeof ctl);
+    if (e == cudaSuccess) e = cudaMemcpy(&ctl, sv->d_ctl, sizeof ctl, cudaMemcpyDeviceToHost);
+    server_free(sv);
+    if (e != cudaSuccess) {
+        set_err(err, errlen, cuda_msg(e, __FILE__, __LINE__));
+        return TD_CUDA_ERROR;
+    }
+    if (ctl.error) {
+        set_err(err, errlen, "serving launch deadline reached");
+        return TD_TIMEOUT;
+    }
+    return TD_OK;
+}
+
+struct td_serve_stats {
+    double p50_ms, p99_ms, p999_ms, mean_ms, max_ms;
+    double offered_per_s, served_per_s, wall_s;
+    double admission_wait_ms_mean;
+    uint64_t served, found;
+    int workers, max_inflight;
+};
+
+// Open-loop experiment: `count` requests (instances[]) arrive as a Poisson
+// process of `rate` per second (seeded); each is admitted when the in-flight
+// frame bytes (max_moves x frame_bytes per request) fit `pool_bytes` and a
+// worker slot is free, then served by the resident launch.  Latency runs from
+// arrival to the host observing the result.  Results land in results[i].
+TD_API int td_serve_open_loop(int device, const td_instance *instances, int count, double rate, uint64_t seed,
+                              uint64_t pool_bytes, unsigned flags, td_result *results, td_serve_stats *stats,
+                              char *err, size_t errlen) {
+    if (count <= 0 || rate <= 0) {
+        set_err(err, errlen, "invalid open-loop arguments");
+        return TD_INVALID_ARG;
+    }
+    void *h = nullptr;
+    const unsigned R = 1u << 16;
+    const double limit_s = std::max(30.0, 4.0 * count / rate + 30.0);
+    int rc = td_serve_open(device, R, flags, limit_s, &h, err, errlen);
+    if (rc != TD_OK) return rc;
+    auto *sv = static_cast<Server *>(h);
+    const size_t frame = sizeof(td_warp_smem) / TD_MAX_DEPTH;
+    const int max_inflight = std::min<int>(sv->workers, (int)R - 1);
+    // Poisson arrivals: exponential gaps from splitmix64 draws
+    std::vector<double> arrive(count);
+    uint64_t st = seed;
+    double t = 0;
+    for (int i = 0; i < count; ++i) {
+        const double u = ((splitmix64(st) >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+        t += -std::log(u) / rate;
+        arrive[i] = t;
+    }
+    std::vector<double> admitted(count, 0), completed(count, 0);
+    std::vector<unsigned long long> ticket(count, 0);
+    std::atomic<int> next_done{0};
+    std::atomic<long long> inflight_bytes{0};
+    std::atomic<int> inflight{0};
+    std::atomic<bool> failed{false};
+    const auto t0 = std::chrono::steady_clock::now();
+    auto now_s = [&] { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
+    std::vector<char> is_done(count, 0);
+    std::atomic<int> submitted{0};
+    std::thread poller([&] {
+        int remaining = count;
+        int lo = 0;
+        while (remaining > 0 && !failed.load()) {
+            const int hi = submitted.load(std::memory_order_acquire);
+            bool progress = false;
+            for (int i = lo; i < hi; ++i) {
+                if (is_done[i]) continue;
+                if (td_serve_poll(h, ticket[i], &results[i])) {
+                    completed[i] = now_s();
+                    is_done[i] = 1;
+                    --remaining;
+                    inflight_bytes.fetch_sub((long long)(instances[i].max_moves * frame));
+                    inflight.fetch_sub(1);
+                    progress = true;
+                }
+            }
+            while (lo < hi && is_done[lo]) ++lo;
+            if (!progress) std::this_thread::yield();
+            if (now_s() > limit_s) failed = true;
+        }
+        next_done = count - remaining;
+    });
+    for (int i = 0; i < count && !failed.load(); ++i) {
+        while (now_s() < arrive[i]) {
+        }
+        const long long need = (long long)(instances[i].max_moves * frame);
+        // a request larger than the pool still runs once nothing else is in flight
+        while (!failed.load() && inflight.load() > 0 &&
+               (inflight.load() >= max_inflight || inflight_bytes.load() + need > (long long)pool_bytes)) {
+        }
+        admitted[i] = now_s();
+        inflight.fetch_add(1);
+        inflight_bytes.fetch_add(need);
+        unsigned long long tk;
+        while (td_serve_submit(h, &instances[i], &tk) != TD_OK && !failed.load()) {
+        }
+        ticket[i] = tk;
+        submitted.store(i + 1, std::memory_order_release);
+    }
+    poller.join();
+    const double wall = now_s();
+    rc = td_serve_close(h, err, errlen);
+    if (failed.load() && rc == TD_OK) {
+        set_err(err, errlen, "open-loop run exceeded its time limit");
+        rc = TD_TIMEOUT;
+    }
+    if (rc != TD_OK) return rc;
+    std::vector<double> lat(count);
+    double wait = 0;
+    uint64_t found = 0;
+    for (int i = 0; i < count; ++i) {
+        lat[i] = (completed[i] - arrive[i]) * 1e3;
+        wait += (admitted[i] - arrive[i]) * 1e3;
+        found += results[i].status == TD_FOUND;
+    }
+    std::vector<double> sorted = lat;
+    std::sort(sorted.begin(), sorted.end());
+    auto pct = [&](double q) { return sorted[std::min<size_t>(sorted.size() - 1, (size_t)(q * (sorted.size() - 1) + 0.5))]; };
+    if (stats) {
+        double sum = 0;
+        for (double v : lat) sum += v;
+        stats->p50_ms = pct(0.50);
+        stats->p99_ms = pct(0.99);
+        stats->p999_ms = pct(0.999);
+        stats->mean_ms = sum / count;
+        stats->max_ms = sorted.back();
+        stats->offered_per_s = count / arrive[count - 1];
+        stats->served_per_s = count / wall;
+        stats->wall_s = wall;
+        stats->admission_wait_ms_mean = wait / count;
+        stats->served = (uint64_t)count;
+        stats->found = found;
+        stats->workers = sv->workers;
+        stats->max_inflight = max_inflight;
+    }
+    return TD_OK;
+}

@@ -10,7 +10,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def test_library_exports_every_declared_symbol(td):
     header = open(os.path.join(ROOT, "include", "td16_b200.h")).read()
-    declared = set(re.findall(r"^\s*(?:int|void|void \*|uint64_t)\s*\*?\s*(td_\w+)\(", header, re.M))
+    declared = set(re.findall(r"^\s*(?:int|void|long long|uint64_t)\s*\*?\s*(td_\w+)\(", header, re.M))
     assert {"td_init_slots", "td_search", "td_search_batch", "td_destroy"} <= declared
     lib = td._lib.lib()
     for name in sorted(declared):

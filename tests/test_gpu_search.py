@@ -205,3 +205,25 @@ def test_work_donation_keeps_verdicts_and_witnesses(slots, oracle):
     _replay_all(oracle, b2, o2, N2, res, 7)
     # expansions of a shared search are summed over every warp that took part
     assert res["expansions"].sum() > 0
+
+
+def test_cuda_graph_replays_match_eager_launches(slots):
+    import torch
+    td = slots
+    perms, n = td.synth_perms(6, 4096, 13, 13, 60, 1, 3)
+    inst = td.prepare_perms(perms, n, 7)
+    eager, _ = td.search_batch(0, inst, 0)
+    d_in = torch.from_numpy(inst.view(np.uint8).copy()).cuda()
+    d_out = torch.zeros(4096 * 32, dtype=torch.uint8, device="cuda")
+    g = td._lib.BatchGraph(0, 4096, d_in.data_ptr(), d_out.data_ptr(), td._lib.FLAG_VERIFY)
+    try:
+        stream = td._lib.lib().td_slot_stream(0)
+        for _ in range(3):
+            d_out.zero_()
+            torch.cuda.synchronize()
+            g.launch(stream)
+            torch.cuda.synchronize()
+            res = d_out.cpu().numpy().view(td.RESULT_DTYPE)
+            assert (res["status"] == eager["status"]).all()  # -6 would mark a witness failing replay
+    finally:
+        g.close()
