@@ -104,7 +104,8 @@ class ClockSampler:
 
 
 def make_instances(td, rank):
-    perms, n = td.synth_perms(SEED ^ (rank << 40), COUNT, 16, 16, 50, 1, 4)
+    from td16_b200.replicas import rank_seed
+    perms, n = td.synth_perms(rank_seed(SEED, rank), COUNT, 16, 16, 50, 1, 4)
     return td.prepare_perms(perms, n, MAX_MOVES), perms, n
 
 
@@ -185,14 +186,19 @@ def run_engine(args):
     d_ok = torch.zeros(count, dtype=torch.uint8, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # larger than the 126 MB L2
 
+    from td16_b200 import autotune
+    tuned = autotune.apply("17")
+
     def step(flags):
         _lib.search_batch_device(0, count, d_in.data_ptr(), d_out.data_ptr(), flags, 0, stream_ptr)
         _lib.validate_batch_device(count, d_in.data_ptr(), d_out.data_ptr(), d_ok.data_ptr(), stream_ptr)
 
+    # one CUDA graph per step: launch epoch, donation engine, device replay
+    graph = _lib.BatchGraph(0, count, d_in.data_ptr(), d_out.data_ptr(), _lib.FLAG_VERIFY)
     for _ in range(args.warmup):
         with torch.cuda.stream(stream):
             flush.zero_()
-        step(0)
+        graph.launch(stream_ptr)
     torch.cuda.synchronize()
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -205,12 +211,12 @@ def run_engine(args):
             with torch.cuda.stream(stream):
                 flush.zero_()
             ev[k][0].record(stream)
-            step(0)
+            graph.launch(stream_ptr)
             ev[k][1].record(stream)
             torch.cuda.synchronize()
             res = d_out.cpu().numpy().view(_lib.RESULT_DTYPE)
-            ok = d_ok.cpu().numpy()
-            verified += int(ok.sum())
+            # a witness that fails the device replay is marked -6, never counted
+            verified += int((res["status"] == 1).sum())
             expansions += int(res["expansions"].astype(np.int64).sum())
             found += int((res["status"] == 1).sum())
             not_found += int((res["status"] == 0).sum())
@@ -219,12 +225,10 @@ def run_engine(args):
     step_ms = [a.elapsed_time(b) for a, b in ev]
     total_s = sum(step_ms) / 1e3
     if dist:
-        t = torch.tensor([total_s], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_s = float(t.item())
-        agg = torch.tensor([verified, expansions, found, not_found, errors], device=dev, dtype=torch.float64)
-        dist.all_reduce(agg)
-        verified, expansions, found, not_found, errors = [int(v) for v in agg.tolist()]
+        from td16_b200 import replicas
+        total_s = replicas.max_over_ranks(total_s, dist, dev)
+        verified, expansions, found, not_found, errors = [
+            int(v) for v in replicas.sum_over_ranks([verified, expansions, found, not_found, errors], dist, dev)]
     value = verified / total_s
 
     # end to end through the public host-buffer API
@@ -273,6 +277,21 @@ def run_engine(args):
         roofline["achieved"] = ach / 1e9
         roofline["frac"] = ach / peak.value
 
+    graph.close()
+    serving = None
+    if world == 1:
+        perms_s, n_s = td.synth_perms(3, 100000, 8, 16, 0, 0, 0)
+        inst_s = td.prepare_perms(perms_s, n_s, (n_s // 2 + 1).astype(np.int32))
+        serving = {"workload": "open-loop Poisson, n uniform 8..16, bound floor(n/2)+1, 64 GiB frame pool"}
+        for rate in (5000.0, 50000.0, 200000.0):
+            try:
+                _, sst = _lib.serve_open_loop(local, inst_s[: int(min(100000, rate * 2))], rate, seed=3)
+                serving[f"{int(rate)}_per_s"] = {k: sst[k] for k in ("p50_ms", "p99_ms", "p999_ms", "served_per_s",
+                                                                     "offered_per_s", "served")}
+            except _lib.TdError as e:
+                serving[f"{int(rate)}_per_s"] = {"error": str(e)}
+        _, bst = td.search_batch(0, inst_s, 0)
+        serving["batched_per_s"] = len(inst_s) / (bst.kernel_ms / 1e3)
     cpu = cpu_baseline() if world == 1 else None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -285,10 +304,12 @@ def run_engine(args):
         "plain_one_launch": {"value": plain_verified / (plain_ms / 1e3), "ms": plain_ms},
         "e2e": {"value": e2e_verified / e2e_s, "unit": UNIT, "h2d_bytes_per_step": count * 16,
                 "d2h_bytes_per_step": count * 32, "ms_per_step": e2e_s / e2e_steps * 1e3},
-        "gpu_launches": args.steps * 2,
+        "gpu_launches": args.steps * 3,
+        "launch_shape": tuned,
         "roofline": roofline,
         "clocks": clocks.summary(),
         "cpu_baseline": cpu,
+        "serving": serving,
     }
     print(json.dumps(line), flush=True)
     if dist:

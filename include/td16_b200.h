@@ -115,6 +115,9 @@ int td_destroy(void);                   /* releases every slot */
 /* Launch shape of the engine (the autotuner's knobs): warps per block and
  * instances per ticket of the ordered persistent kernel. */
 int td_configure(int warps_per_block, int grain);
+/* Deadline of every later launch in seconds (default TD16_TIME_LIMIT_S or
+ * 300): searches and device waits that pass it end with a timeout status. */
+int td_set_time_limit(double seconds);
 /* Work donation of the free-order engine: items per donation, deepest level
  * whose children may be donated, expansions between idle checks. */
 int td_configure_steal(int grain, int split_level, int check_every);
@@ -237,6 +240,19 @@ void *td_cert_writer_open(const char *path, double flush_seconds);
 int td_cert_writer_enqueue(void *writer, const uint8_t *omega, int n,
                            const uint8_t *abc, int count);
 long long td_cert_writer_close(void *writer);
+
+/* Queues the found witnesses of a batch (caller pairs, stride 17) as
+ * certificates; returns the number queued. */
+long long td_cert_writer_enqueue_batch(void *writer, int count, const uint8_t *beta,
+                                       const uint8_t *omega, const uint8_t *n,
+                                       const td_result *results);
+/* Reads a certificate file for n-symbol domains: omega (stride 17), symbol
+ * triples (stride 27), move counts.  Returns the record count or -1. */
+long long td_cert_read_file(const char *path, int n, long long cap, uint8_t *omega,
+                            uint8_t *abc, uint8_t *depth);
+/* Caller pairs of S_n permutations: beta = (0..n), omega (stride 17). */
+void td_pairs_from_perms(int count, const int8_t *perms, const uint8_t *n,
+                         uint8_t *beta, uint8_t *omega);
 
 /* Position triples -> symbol triples on a copy of beta
  * (GPUSortingSearch.java:229-238). */

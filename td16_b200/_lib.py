@@ -52,11 +52,11 @@ _lib = None
 EXPORTS = ["td_init_slots", "td_search", "td_search_ordered", "td_slot_count", "td_slot_device",
            "td_slot_stream", "td_destroy", "td_prepare_pairs", "td_prepare_perms", "td_synth_perms",
            "td_search_batch", "td_search_batch_device", "td_validate_batch_device",
-           "td_positions_to_symbols", "td_configure", "td_configure_steal", "td_int_issue_peak",
+           "td_positions_to_symbols", "td_configure", "td_configure_steal", "td_set_time_limit", "td_int_issue_peak",
            "td_codec_key", "td_codec_value", "td_codec_decode_key", "td_codec_decode_value",
            "td_replay_symbols_device", "td_cert_writer_open", "td_cert_writer_enqueue", "td_cert_writer_close",
            "td_serve_open", "td_serve_workers", "td_serve_submit", "td_serve_poll", "td_serve_close",
-           "td_serve_open_loop", "td_batch_graph_create", "td_batch_graph_launch", "td_batch_graph_destroy"]
+           "td_serve_open_loop", "td_cert_writer_enqueue_batch", "td_cert_read_file", "td_pairs_from_perms", "td_batch_graph_create", "td_batch_graph_launch", "td_batch_graph_destroy"]
 
 
 def lib():
@@ -88,6 +88,7 @@ def lib():
     L.td_positions_to_symbols.restype = None
     L.td_configure.argtypes = [C.c_int, C.c_int]
     L.td_configure_steal.argtypes = [C.c_int, C.c_int, C.c_int]
+    L.td_set_time_limit.argtypes = [C.c_double]
     L.td_codec_key.argtypes = [vp, C.c_int, vp, C.c_int]
     L.td_codec_value.argtypes = [vp, C.c_int, vp, C.c_int]
     L.td_codec_decode_key.argtypes = [vp, C.c_int, C.c_int, vp]
@@ -101,6 +102,12 @@ def lib():
     L.td_batch_graph_create.argtypes = [C.c_int, C.c_int, vp, vp, C.c_uint, C.c_uint64, C.POINTER(vp), cp, sz]
     L.td_batch_graph_launch.argtypes = [vp, vp, cp, sz]
     L.td_batch_graph_destroy.argtypes = [vp]
+    L.td_cert_writer_enqueue_batch.argtypes = [vp, C.c_int, vp, vp, vp, vp]
+    L.td_cert_writer_enqueue_batch.restype = C.c_longlong
+    L.td_cert_read_file.argtypes = [cp, C.c_int, C.c_longlong, vp, vp, vp]
+    L.td_cert_read_file.restype = C.c_longlong
+    L.td_pairs_from_perms.argtypes = [C.c_int, vp, vp, vp, vp]
+    L.td_pairs_from_perms.restype = None
     L.td_serve_open.argtypes = [C.c_int, C.c_uint, C.c_uint, C.c_double, C.POINTER(vp), cp, sz]
     L.td_serve_workers.argtypes = [vp]
     L.td_serve_submit.argtypes = [vp, vp, C.POINTER(C.c_ulonglong)]
@@ -233,6 +240,11 @@ def positions_to_symbols(beta, moves):
 def configure(warps_per_block: int, grain: int) -> None:
     if lib().td_configure(int(warps_per_block), int(grain)) != OK:
         raise TdError(INVALID_ARG, "invalid launch configuration")
+
+
+def set_time_limit(seconds: float) -> None:
+    if lib().td_set_time_limit(float(seconds)) != OK:
+        raise TdError(INVALID_ARG, "time limit must be positive")
 
 
 def configure_steal(grain: int, split_level: int, check_every: int) -> None:

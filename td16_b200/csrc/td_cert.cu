@@ -24,6 +24,8 @@
 #include <vector>
 
 #define TD_API extern "C" __attribute__((visibility("default")))
+
+#include "td_core.cuh"
 #define TD_CERT_MAX_N 17
 #define TD_CERT_MAX_MOVES 9
 
@@ -257,4 +259,92 @@ TD_API long long td_cert_writer_close(void *handle) {
     const long long n = (long long)w->written;
     delete w;
     return failed ? -2 : n;
+}
+
+// Queues the found witnesses of a batch: omega/beta stride 17 (the caller's
+// pair), n symbols each, results as td_result records (caller positions).
+// Returns the number queued, -1 for an unencodable record, -2 after a write
+// failure.
+TD_API long long td_cert_writer_enqueue_batch(void *handle, int count, const uint8_t *beta, const uint8_t *omega,
+                                              const uint8_t *n, const td_result *results) {
+    auto *w = static_cast<CertWriter *>(handle);
+    if (!w) return -1;
+    std::deque<std::vector<uint8_t>> recs;
+    for (int i = 0; i < count; ++i) {
+        const td_result &r = results[i];
+        if (r.status != TD_FOUND || r.depth <= 0 || r.depth > TD_CERT_MAX_MOVES) continue;
+        const int N = n[i];
+        uint8_t cur[TD_CERT_MAX_N], nxt[TD_CERT_MAX_N], abc[3 * TD_CERT_MAX_MOVES];
+        std::memcpy(cur, beta + (size_t)i * TD_CERT_MAX_N, (size_t)N);
+        for (int d = 0; d < r.depth; ++d) {  // GPUSortingSearch.java:229-238
+            const int a = r.moves[d] & 31, b = (r.moves[d] >> 5) & 31, c = (r.moves[d] >> 10) & 31;
+            if (!(a < b && b < c && c < N)) return -1;
+            abc[3 * d] = cur[a];
+            abc[3 * d + 1] = cur[b];
+            abc[3 * d + 2] = cur[c];
+            int k = 0;
+            for (int x = 0; x < a; ++x) nxt[k++] = cur[x];
+            for (int x = b; x < c; ++x) nxt[k++] = cur[x];
+            for (int x = a; x < b; ++x) nxt[k++] = cur[x];
+            for (int x = c; x < N; ++x) nxt[k++] = cur[x];
+            std::memcpy(cur, nxt, (size_t)N);
+        }
+        uint8_t key[32], val[64];
+        const int kl = td_codec_key(omega + (size_t)i * TD_CERT_MAX_N, N, key, sizeof key);
+        const int vl = td_codec_value(abc, r.depth, val, sizeof val);
+        if (kl < 0 || vl < 0) return -1;
+        std::vector<uint8_t> rec(2 + kl + vl);
+        rec[0] = (uint8_t)kl;
+        rec[1] = (uint8_t)vl;
+        std::memcpy(&rec[2], key, kl);
+        std::memcpy(&rec[2 + kl], val, vl);
+        recs.push_back(std::move(rec));
+    }
+    std::lock_guard<std::mutex> g(w->mu);
+    if (w->failed) return -2;
+    const long long q = (long long)recs.size();
+    for (auto &r : recs) w->q.push_back(std::move(r));
+    w->cv.notify_one();
+    return q;
+}
+
+// Reads up to `cap` records of a certificate file written for domains of n
+// symbols into omega (stride 17), abc (stride 27) and depth.  Returns the
+// number read, or -1 for a malformed record.
+TD_API long long td_cert_read_file(const char *path, int n, long long cap, uint8_t *omega, uint8_t *abc,
+                                   uint8_t *depth) {
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return -1;
+    long long k = 0;
+    uint8_t hdr[2], buf[96];
+    while (k < cap && std::fread(hdr, 1, 2, f) == 2) {
+        const int kl = hdr[0], vl = hdr[1];
+        if (kl + vl > (int)sizeof buf || std::fread(buf, 1, (size_t)(kl + vl), f) != (size_t)(kl + vl)) {
+            std::fclose(f);
+            return -1;
+        }
+        if (td_codec_decode_key(buf, kl, n, omega + (size_t)k * TD_CERT_MAX_N) < 0) {
+            std::fclose(f);
+            return -1;
+        }
+        const int m = td_codec_decode_value(buf + kl, vl, abc + (size_t)k * 27, TD_CERT_MAX_MOVES);
+        if (m < 0) {
+            std::fclose(f);
+            return -1;
+        }
+        depth[k] = (uint8_t)m;
+        ++k;
+    }
+    std::fclose(f);
+    return k;
+}
+
+// Caller pairs of S_n permutations (perms int8 stride 16): beta = (0..n),
+// omega one-line over n+1 symbols (stride 17).
+TD_API void td_pairs_from_perms(int count, const int8_t *perms, const uint8_t *n, uint8_t *beta, uint8_t *omega) {
+    for (int i = 0; i < count; ++i) {
+        int init;
+        td_perm_to_pair(perms + (size_t)i * 16, n[i], beta + (size_t)i * TD_CERT_MAX_N,
+                        omega + (size_t)i * TD_CERT_MAX_N, &init);
+    }
 }

@@ -128,12 +128,12 @@ TD_HD void td_apply_move(uint64_t L, int off, int N, int i, int j, int k,
 // A triple (i,j,k) reads entries (i,j), (j,k), (k,i) and forms a 12-bit index
 // into a table that restates delta_even_cycles (sorting_search.cu:240-332) and
 // the move filter (:375-380, :607-610).  Table values: 0 = filtered out,
-// 4 = odd-cycle change 0, 12 = change +2 (multiples of 4 so the value is the
-// shift into the per-node outcome word).
+// 1 = odd-cycle change 0, 2 = change +2.  The value is the byte of the
+// per-node outcome word that holds that class's flags (byte 0 is zero).
 
 #define TD_CLASS_SKIP 0
-#define TD_CLASS_ZERO 4
-#define TD_CLASS_PLUS2 12
+#define TD_CLASS_ZERO 1
+#define TD_CLASS_PLUS2 2
 
 TD_HD int td_class_of_index(int idx) {
     const int S1 = idx & 1, P1 = (idx >> 1) & 1, G1 = (idx >> 2) & 1, O1 = (idx >> 3) & 1;  // (a,b)

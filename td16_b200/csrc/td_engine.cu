@@ -54,8 +54,13 @@ static_assert(sizeof(td_result) == 32, "td_result layout");
 
 #define TD_LUT_BYTES 4096
 
+// Class table (td_class_of_index for every 12-bit index), filled by the host.
+__device__ __align__(16) uint8_t td_lut_global[TD_LUT_BYTES];
+
 __device__ __forceinline__ void td_block_init(uint8_t *lut, td_warp_smem *ws, int warps) {
-    for (int i = threadIdx.x; i < TD_LUT_BYTES; i += blockDim.x) lut[i] = (uint8_t)td_class_of_index(i);
+    const uint4 *src = reinterpret_cast<const uint4 *>(td_lut_global);
+    uint4 *dst = reinterpret_cast<uint4 *>(lut);
+    for (int i = threadIdx.x; i < TD_LUT_BYTES / 16; i += blockDim.x) dst[i] = src[i];
     for (int w = 0; w < warps; ++w)
         for (int b = threadIdx.x; b < TD_PT_STRIDE; b += blockDim.x) ws[w].pt[TD_PT_DUMMY + b] = 0;
     __syncthreads();
@@ -182,7 +187,11 @@ __global__ void __launch_bounds__(256) td_steal_kernel(const td_instance *__rest
     for (;;) {
         int kind = 0, unit = -1;
         if (lane == 0) {
-            atomicAdd(&pool->active, 1);
+            // `active` counts warps that hold a unit.  Counting claim attempts
+            // as well would let idle warps keep it above zero forever.  A warp
+            // that holds a unit but is not counted yet can only let others
+            // leave early; it finishes its unit itself, and it donates only to
+            // warps still waiting, so no work is left behind.
             if (*(volatile int *)&pool->inst_ticket < count) {
                 const int t = atomicAdd(&pool->inst_ticket, 1);
                 if (t < count) { kind = 1; unit = t; }
@@ -196,7 +205,7 @@ __global__ void __launch_bounds__(256) td_steal_kernel(const td_instance *__rest
                     C = prev;
                 }
             }
-            if (!kind) atomicSub(&pool->active, 1);
+            if (kind) atomicAdd(&pool->active, 1);
         }
         kind = __shfl_sync(TD_FULL, kind, 0);
         unit = __shfl_sync(TD_FULL, unit, 0);
@@ -215,8 +224,10 @@ __global__ void __launch_bounds__(256) td_steal_kernel(const td_instance *__rest
                 }
             }
             if (__shfl_sync(TD_FULL, done, 0)) break;
+            // waiting warps back off to 32 us so that their counter reads do
+            // not crowd the L2 slices the busy warps' atomics go to
             __nanosleep(backoff);
-            backoff = min(backoff * 2u, 8192u);
+            backoff = min(backoff * 2u, 32768u);
             continue;
         }
         if (lane == 0 && idle) { atomicSub(&pool->idle, 1); idle = false; }
@@ -415,13 +426,17 @@ std::string cuda_msg(cudaError_t e, const char *file, int line) {
 
 size_t smem_bytes(int warps) { return TD_LUT_BYTES + (size_t)warps * sizeof(td_warp_smem); }
 
+std::atomic<uint64_t> g_time_limit_ns{0};
+
+// Launch deadline: td_set_time_limit, else TD16_TIME_LIMIT_S, else 300 s.
 uint64_t time_limit_ns() {
-    static uint64_t v = [] {
-        const char *s = std::getenv("TD16_TIME_LIMIT_S");
-        double secs = s ? std::atof(s) : 300.0;
-        if (!(secs > 0)) secs = 300.0;
-        return (uint64_t)(secs * 1e9);
-    }();
+    uint64_t v = g_time_limit_ns.load(std::memory_order_relaxed);
+    if (v) return v;
+    const char *s = std::getenv("TD16_TIME_LIMIT_S");
+    double secs = s ? std::atof(s) : 300.0;
+    if (!(secs > 0)) secs = 300.0;
+    v = (uint64_t)(secs * 1e9);
+    g_time_limit_ns.store(v, std::memory_order_relaxed);
     return v;
 }
 
@@ -438,6 +453,9 @@ int ensure_device(int device, char *err, size_t errlen) {
                 for (int k = j + 1; k < N; ++k) tri[base + t++] = td_pack_move(i, j, k);
     }
     TD_CHECK(cudaMemcpyToSymbol(td_tri_table, tri.data(), tri.size() * sizeof(uint16_t)));
+    std::vector<uint8_t> lut(TD_LUT_BYTES);
+    for (int i = 0; i < TD_LUT_BYTES; ++i) lut[i] = (uint8_t)td_class_of_index(i);
+    TD_CHECK(cudaMemcpyToSymbol(td_lut_global, lut.data(), lut.size()));
     TD_CHECK(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device));
     const int max_warps = 8;
     const size_t max_smem = smem_bytes(max_warps);
@@ -780,6 +798,14 @@ TD_API int td_configure(int warps_per_block, int grain) {
     g_warps_per_block = warps_per_block;
     g_grain = grain;
     for (auto &d : g_dev) d.blocks_per_sm = d.steal_blocks_per_sm = 0;
+    return TD_OK;
+}
+
+// Sets the deadline of every later launch (seconds > 0); every device wait
+// and search ends with a timeout status once it passes.
+TD_API int td_set_time_limit(double seconds) {
+    if (!(seconds > 0)) return TD_INVALID_ARG;
+    g_time_limit_ns.store((uint64_t)(seconds * 1e9), std::memory_order_relaxed);
     return TD_OK;
 }
 

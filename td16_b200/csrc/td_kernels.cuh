@@ -19,24 +19,34 @@
 #define TD_PT_ROWS 18          // 17 position rows + one zero row for idle lanes
 #define TD_PT_DUMMY (17 * TD_PT_STRIDE)
 #define TD_TRI_TABLE 3060      // sum over N <= 17 of C(N,3) = C(18,4)
+#define TD_G0 0x09249249u      // bit 0 of each 3-bit group
+#define TD_G1 0x12492492u      // bit 1 of each group
+#define TD_G2 0x24924924u      // bit 2 of each group
+
+// floor(b / 3) for 0 <= b <= 29: the step of a bit inside a packed word
+__device__ __forceinline__ int td_group_of(int b) { return (b * 11) >> 5; }
 
 // Per-warp shared state.
 struct td_warp_smem {
     uint8_t pt[TD_PT_ROWS * TD_PT_STRIDE];     // pair table of the current node
-    uint32_t m1[TD_MAX_DEPTH][32];             // per level, per lane step masks
-    uint32_t m2[TD_MAX_DEPTH][32];
+    // per level, per lane: the outcome of every step in 3-bit groups, ten
+    // steps per word (step st in word st/10 at bit 3*(st%10)): bit 0 found
+    // (accepted root in ordered mode), bit 1 first-choice child, bit 2
+    // second-choice child
+    uint32_t pm[TD_MAX_DEPTH][3][32];
     uint64_t L[TD_MAX_DEPTH + 1];              // pinned state per level
     uint32_t acc[TD_MAX_DEPTH + 2];            // accept mask over odd counts, per depth
     uint32_t reach[TD_MAX_DEPTH + 2];          // prune mask over odd counts, per depth
     uint16_t path[TD_MAX_DEPTH];               // caller-position move per level
     uint8_t off[TD_MAX_DEPTH + 1];
-    alignas(16) uint16_t md[24];               // cycle descriptor by caller position
+    alignas(16) uint8_t lead[32];              // cycle leader by caller position
+    alignas(16) uint8_t dist[32];              // omega steps to the leader
 };
 
 // Lexicographic position triples i|j<<5|k<<10 for every N, at offset C(N,4).
 __device__ uint16_t td_tri_table[TD_TRI_TABLE];
 
-__device__ __forceinline__ int td_tri_base(int N) {
+TD_HD int td_tri_base(int N) {
     return N < 4 ? 0 : N * (N - 1) * (N - 2) * (N - 3) / 24;
 }
 
@@ -99,43 +109,40 @@ __device__ __forceinline__ int td_prepare_node(td_warp_smem &s, uint64_t L, int 
     const int after_leader = __shfl_sync(TD_FULL, nx, m);
     const int len = __shfl_sync(TD_FULL, d, after_leader) + 1;
     const int odd = __popc(__ballot_sync(TD_FULL, act && leader && (len & 1)));
-    // descriptors by caller position: md = leader | dist << 5
+    // descriptors by caller position, one byte each
     int rp = p - off;
     rp += rp < 0 ? N : 0;
-    const uint32_t md = (uint32_t)m | ((uint32_t)d << 5);
-    if (act) s.md[rp] = (uint16_t)md;
-    __syncwarp();
-    uint16_t mdq[24];
-    {
-        const uint4 *src = reinterpret_cast<const uint4 *>(s.md);
-        uint4 v0 = src[0], v1 = src[1], v2 = src[2];
-        const uint32_t w[12] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w, v2.x, v2.y, v2.z, v2.w};
-#pragma unroll
-        for (int k = 0; k < 12; ++k) {
-            mdq[2 * k] = (uint16_t)(w[k] & 0xffffu);
-            mdq[2 * k + 1] = (uint16_t)(w[k] >> 16);
-        }
+    if (act) {
+        s.lead[rp] = (uint8_t)m;
+        s.dist[rp] = (uint8_t)d;
     }
-    // pair table row of this lane's caller position
-    const uint32_t o3 = (uint32_t)(len & 1) << 3;
-    const uint32_t fixed4 = len == 1 ? 4u : 0u;
+    __syncwarp();
+    // pair table row of this lane's caller position, four entries per word
+    // (byte-SIMD: every byte stays below 0x80, so no borrow crosses a byte)
+    const uint32_t H = 0x80808080u, ONE = 0x01010101u;
+    const uint32_t Mp = (uint32_t)m * ONE, Dp = (uint32_t)d * ONE;
+    const uint32_t O8 = (len & 1) ? 0x08080808u : 0u;
+    const uint32_t F4 = len == 1 ? 0x04040404u : 0u;
+    const uint32_t Lodd = (len & 1) ? ONE : 0u;
+    const uint4 ml = *reinterpret_cast<const uint4 *>(s.lead);
+    const uint4 dl = *reinterpret_cast<const uint4 *>(s.dist);
+    const uint32_t m4 = *reinterpret_cast<const uint32_t *>(s.lead + 16);
+    const uint32_t d4 = *reinterpret_cast<const uint32_t *>(s.dist + 16);
+    const uint32_t Mw[5] = {ml.x, ml.y, ml.z, ml.w, m4};
+    const uint32_t Dw[5] = {dl.x, dl.y, dl.z, dl.w, d4};
     uint32_t row[5];
 #pragma unroll
-    for (int k = 0; k < 5; ++k) row[k] = 0;
-#pragma unroll
-    for (int rq = 0; rq < TD_MAX_N; ++rq) {
-        const uint32_t q = mdq[rq];
-        const uint32_t x = md ^ q;
-        uint32_t e;
-        if ((x & 31u) == 0) {
-            const uint32_t g = md > q ? 1u : 0u;   // same leader: compares dist
-            uint32_t w = (x >> 5) & 1u;            // parity of the dist difference
-            w ^= (o3 >> 3) & (g ^ 1u);             // wrap of an odd cycle flips it
-            e = 1u | (w << 1) | (g << 2) | o3;
-        } else {
-            e = fixed4 | o3;
-        }
-        row[rq >> 2] |= e << (8 * (rq & 3));
+    for (int k = 0; k < 5; ++k) {
+        const uint32_t xm = (Mw[k] ^ Mp) | H;
+        const uint32_t same = ~(xm - ONE) & H;                          // 0x80 where leaders match
+        const uint32_t gt = ((Dp | H) - Dw[k] - ONE) & H;               // 0x80 where dist_p > dist_q
+        const uint32_t G = gt >> 7;
+        uint32_t P = (Dp ^ Dw[k]) & ONE;                                // parity of the dist difference
+        P ^= (G ^ ONE) & Lodd;                                          // wrap of an odd cycle flips it
+        const uint32_t sel = (same << 1) - (same >> 7);                 // 0xff in bytes with the same leader
+        const uint32_t in_cycle = ONE | (P << 1) | (G << 2) | O8;
+        const uint32_t apart = F4 | O8;
+        row[k] = (in_cycle & sel) | (apart & ~sel);
     }
     if (act) {
         uint32_t *dst = reinterpret_cast<uint32_t *>(&s.pt[rp * TD_PT_STRIDE]);
@@ -145,19 +152,32 @@ __device__ __forceinline__ int td_prepare_node(td_warp_smem &s, uint64_t L, int 
     return odd;
 }
 
-// Accept / prune masks of one instance (lane o evaluates odd count o).
+// Accept / prune masks of one instance: lane D computes the masks of depth D
+// over all odd counts.  With full sorting the accept test only passes at
+// odd == N and its f32 rate part depends on D alone, and the prune bound
+// D + ceil((N - odd)/2) <= maxDepth is a threshold on odd, so both masks take
+// one f32 division per lane.  Partial sorting evaluates every odd count.
 __device__ __forceinline__ void td_rate_masks(td_warp_smem &s, const td_instance &x) {
-    const int o = threadIdx.x & 31;
+    const int D = threadIdx.x & 31;
     const int N = x.n_symbols, init = td_inst_init(x), full = td_inst_full(x);
     const int maxd = x.max_moves;
-#pragma unroll 1
-    for (int D = 0; D <= TD_MAX_DEPTH + 1; ++D) {
-        const unsigned a = __ballot_sync(TD_FULL, td_accepts(N, init, x.min_rate, full, o, D));
-        const unsigned r = __ballot_sync(TD_FULL, D < maxd && td_can_reach(N, init, x.min_rate, maxd, full, o, D));
-        if (o == 0) {
-            s.acc[D] = a;
-            s.reach[D] = r;
+    uint32_t a = 0, r = 0;
+    if (D <= TD_MAX_DEPTH + 1) {
+        if (full) {
+            if (td_accepts(N, init, x.min_rate, 1, N, D)) a = 1u << N;
+            if (D < maxd) {
+                // D + (N - odd + 1) / 2 <= maxd  <=>  odd >= N - 2 * (maxd - D)
+                const int lo = N - 2 * (maxd - D);
+                r = lo <= 0 ? 0xffffffffu : (0xffffffffu << lo);
+            }
+        } else {
+            for (int o = 0; o < 32; ++o) {
+                if (td_accepts(N, init, x.min_rate, 0, o, D)) a |= 1u << o;
+                if (D < maxd && td_can_reach(N, init, x.min_rate, maxd, 0, o, D)) r |= 1u << o;
+            }
         }
+        s.acc[D] = a;
+        s.reach[D] = r;
     }
     __syncwarp();
 }
@@ -174,8 +194,8 @@ __device__ __forceinline__ uint64_t td_globaltimer() {
     return t;
 }
 
-// Evaluate all children of the node at `level`.  Fills the level's masks and
-// returns the found child's u, or -1.
+// Evaluate all children of the node at `level`.  Fills the level's packed
+// outcome words and returns the found child's u, or -1.
 template <bool ORDERED>
 __device__ __forceinline__ int td_evaluate(td_warp_smem &s, const uint8_t *lut,
                                            const uint32_t (&code)[TD_MAX_STEPS], int steps,
@@ -186,12 +206,13 @@ __device__ __forceinline__ int td_evaluate(td_warp_smem &s, const uint8_t *lut,
     const uint32_t f0 = (accD >> odd) & 1u, f2 = (accD >> (odd + 2)) & 1u;
     const uint32_t x0 = ((reachD >> odd) & 1u) & (f0 ^ 1u);
     const uint32_t x2 = ((reachD >> (odd + 2)) & 1u) & (f2 ^ 1u);
-    const uint32_t nt = ORDERED
-        ? (((f0 | (x0 << 1)) << TD_CLASS_ZERO) | ((f2 | (x2 << 1)) << TD_CLASS_PLUS2))
-        : (((f0 | (x0 << 2)) << TD_CLASS_ZERO) | ((f2 | (x2 << 1)) << TD_CLASS_PLUS2));
+    // byte c of nt holds the flags of class c; byte 0 (filtered out) is zero
+    const uint32_t flags0 = ORDERED ? (f0 | (x0 << 1)) : (f0 | (x0 << 2));
+    const uint32_t flags2 = f2 | (x2 << 1);
+    const uint32_t nt = (flags0 << (8 * TD_CLASS_ZERO)) | (flags2 << (8 * TD_CLASS_PLUS2));
     (void)maxd;
     __syncwarp();
-    uint32_t fb = 0, w1 = 0, w2 = 0;
+    uint32_t P0 = 0, P1 = 0, P2 = 0;
 #pragma unroll
     for (int st = 0; st < TD_MAX_STEPS; ++st) {
         if (st < steps) {
@@ -200,21 +221,24 @@ __device__ __forceinline__ int td_evaluate(td_warp_smem &s, const uint8_t *lut,
             const uint32_t B = s.pt[(c >> 10) & 1023u];
             const uint32_t C = s.pt[c >> 20];
             const uint32_t cls = lut[A | (B << 4) | (C << 8)];
-            const uint32_t tb = nt >> cls;
-            fb |= (tb & 1u) << st;
-            w1 |= ((tb >> 1) & 1u) << st;
-            if (!ORDERED) w2 |= ((tb >> 2) & 1u) << st;
+            const uint32_t tb = __byte_perm(nt, 0, cls);  // flags of this child's class
+            const uint32_t mul = 1u << (3 * (st % 10));
+            if (st < 10) P0 += tb * mul;
+            else if (st < 20) P1 += tb * mul;
+            else P2 += tb * mul;
         }
     }
-    if (ORDERED && level == 0) {  // roots are accepted on visit, not on seeding
-        s.m1[0][lane] = w1;
-        s.m2[0][lane] = fb;
-        return -1;
-    }
-    s.m1[level][lane] = w1;
-    if (!ORDERED) s.m2[level][lane] = w2;
-    if (__any_sync(TD_FULL, fb != 0)) {
-        const uint32_t key = fb ? ((uint32_t)(__ffs(fb) - 1) << 5) | (uint32_t)lane : 0xffffffffu;
+    s.pm[level][0][lane] = P0;
+    s.pm[level][1][lane] = P1;
+    s.pm[level][2][lane] = P2;
+    if (ORDERED && level == 0) return -1;  // roots are accepted on visit, not on seeding
+    const uint32_t q0 = P0 & TD_G0, q1 = P1 & TD_G0, q2 = P2 & TD_G0;
+    if (__any_sync(TD_FULL, (q0 | q1 | q2) != 0)) {
+        int st = -1;
+        if (q0) st = td_group_of(__ffs(q0) - 1);
+        else if (q1) st = 10 + td_group_of(__ffs(q1) - 1);
+        else if (q2) st = 20 + td_group_of(__ffs(q2) - 1);
+        const uint32_t key = st >= 0 ? ((uint32_t)st << 5) | (uint32_t)lane : 0xffffffffu;
         return (int)__reduce_min_sync(TD_FULL, key);
     }
     return -1;
@@ -225,37 +249,33 @@ __device__ __forceinline__ int td_evaluate(td_warp_smem &s, const uint8_t *lut,
 template <bool ORDERED>
 __device__ __forceinline__ int td_next_child(td_warp_smem &s, int level, int *accepted) {
     const int lane = threadIdx.x & 31;
-    uint32_t a1 = s.m1[level][lane];
-    uint32_t a2 = ORDERED ? (level == 0 ? s.m2[0][lane] : 0u) : s.m2[level][lane];
+    const uint32_t P0 = s.pm[level][0][lane], P1 = s.pm[level][1][lane], P2 = s.pm[level][2][lane];
     const bool desc_lanes = ORDERED && level > 0;
-    uint32_t w;
-    bool use1 = true;
+    uint32_t cm;
     if (ORDERED) {
-        w = a1 | a2;
+        cm = level == 0 ? (TD_G0 | TD_G1) : TD_G1;
     } else {
-        use1 = __any_sync(TD_FULL, a1 != 0);
-        w = use1 ? a1 : a2;
+        const bool any1 = __any_sync(TD_FULL, ((P0 | P1 | P2) & TD_G1) != 0);
+        cm = any1 ? TD_G1 : TD_G2;  // +2 children first
     }
+    const uint32_t w0 = P0 & cm, w1 = P1 & cm, w2 = P2 & cm;
+    int st = -1;
+    if (w2) st = 20 + td_group_of(31 - __clz(w2));
+    else if (w1) st = 10 + td_group_of(31 - __clz(w1));
+    else if (w0) st = td_group_of(31 - __clz(w0));
     uint32_t key = 0;
-    if (w) key = ((31u - __clz(w)) << 5) + (uint32_t)(desc_lanes ? 31 - lane : lane) + 1u;
+    if (st >= 0) key = ((uint32_t)st << 5) + (uint32_t)(desc_lanes ? 31 - lane : lane) + 1u;
     key = __reduce_max_sync(TD_FULL, key);
     *accepted = 0;
     if (key == 0) return -1;
     key -= 1;
-    const int st = (int)(key >> 5);
+    st = (int)(key >> 5);
     const int win = desc_lanes ? 31 - (int)(key & 31) : (int)(key & 31);
-    const uint32_t bit = 1u << st;
-    if (ORDERED && level == 0) *accepted = __shfl_sync(TD_FULL, (a2 & bit) ? 1 : 0, win);
-    if (lane == win) {
-        if (ORDERED) {
-            s.m1[level][lane] = a1 & ~bit;
-            if (level == 0) s.m2[0][lane] = a2 & ~bit;
-        } else if (use1) {
-            s.m1[level][lane] = a1 & ~bit;
-        } else {
-            s.m2[level][lane] = a2 & ~bit;
-        }
-    }
+    const int k = st < 10 ? 0 : (st < 20 ? 1 : 2);
+    const int j = st - 10 * k;
+    const uint32_t Pk = k == 0 ? P0 : (k == 1 ? P1 : P2);
+    if (ORDERED && level == 0) *accepted = __shfl_sync(TD_FULL, (int)((Pk >> (3 * j)) & 1u), win);
+    if (lane == win) s.pm[level][k][lane] = Pk & ~(7u << (3 * j));
     __syncwarp();
     return st * 32 + win;
 }
@@ -322,26 +342,27 @@ struct td_dfs_out {
 __device__ __forceinline__ int td_donate(td_warp_smem &s, const td_donate_ctx &dc, int d0, int level, int N,
                                          int T, int tri_base, int want) {
     const int lane = threadIdx.x & 31;
+    const uint32_t CAND = TD_G1 | TD_G2;
     int lv = -1;
     for (int l = d0; l <= level && l <= dc.max_level; ++l) {
-        const uint32_t w = s.m1[l][lane] | s.m2[l][lane];
+        const uint32_t w = (s.pm[l][0][lane] | s.pm[l][1][lane] | s.pm[l][2][lane]) & CAND;
         if (__any_sync(TD_FULL, w != 0)) { lv = l; break; }
     }
     if (lv < 0) return 0;
+    uint32_t P0 = s.pm[lv][0][lane], P1 = s.pm[lv][1][lane], P2 = s.pm[lv][2][lane];
+    uint32_t Q0 = P0 & CAND, Q1 = P1 & CAND, Q2 = P2 & CAND;
+    const int cnt = __popc(Q0) + __popc(Q1) + __popc(Q2);
+    const int have = __reduce_add_sync(TD_FULL, (unsigned)cnt);
     // leave at least one child to this warp when the level is the current one
-    uint32_t w1 = s.m1[lv][lane], w2 = s.m2[lv][lane];
-    const int have = __reduce_add_sync(TD_FULL, (unsigned)(__popc(w1) + __popc(w2)));
-    int give = min(want, have - (lv == level ? 1 : 0));
+    const int give = min(want, have - (lv == level ? 1 : 0));
     if (give <= 0) return 0;
-    // take the lowest lanes' bits first: lane l gives up to `mine` children
-    const int cnt = __popc(w1) + __popc(w2);
-    int before = cnt;
+    int before = cnt;  // lanes give in lane order
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const int v = __shfl_up_sync(TD_FULL, before, o);
         if (lane >= o) before += v;
     }
-    before -= cnt;  // exclusive prefix
+    before -= cnt;
     const int mine = max(0, min(cnt, give - before));
     // reserve `give` item slots; the count never passes the capacity and never
     // goes back, so a taker only ever claims slots that a donor will write
@@ -365,10 +386,16 @@ __device__ __forceinline__ int td_donate(td_warp_smem &s, const td_donate_ctx &d
     }
     int slot = base + before;
     for (int taken = 0; taken < mine; ++taken) {
-        uint32_t *wp = w1 ? &w1 : &w2;
-        const int st = __ffs(*wp) - 1;
-        *wp &= *wp - 1;
-        const int u = 32 * st + lane;
+        int k, b;
+        if (Q0) { k = 0; b = __ffs(Q0) - 1; Q0 &= Q0 - 1; }
+        else if (Q1) { k = 1; b = __ffs(Q1) - 1; Q1 &= Q1 - 1; }
+        else { k = 2; b = __ffs(Q2) - 1; Q2 &= Q2 - 1; }
+        const int j = td_group_of(b);
+        const uint32_t clear = ~(7u << (3 * j));
+        if (k == 0) P0 &= clear;
+        else if (k == 1) P1 &= clear;
+        else P2 &= clear;
+        const int u = 32 * (10 * k + j) + lane;
         const uint32_t t = td_tri_table[tri_base + T - 1 - u];
         uint64_t nL;
         int noff;
@@ -385,8 +412,9 @@ __device__ __forceinline__ int td_donate(td_warp_smem &s, const td_donate_ctx &d
         atomicExch(&dc.ready[slot], dc.epoch);
         ++slot;
     }
-    s.m1[lv][lane] = w1;
-    s.m2[lv][lane] = w2;
+    s.pm[lv][0][lane] = P0;
+    s.pm[lv][1][lane] = P1;
+    s.pm[lv][2][lane] = P2;
     __syncwarp();
     return give;
 }

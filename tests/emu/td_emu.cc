@@ -67,9 +67,9 @@ int evaluate(Emu &e, int level, int odd) {
     const int f0 = (e.acc[D] >> odd) & 1, f2 = (e.acc[D] >> (odd + 2)) & 1;
     const int x0 = (D < e.maxd) && ((e.reach[D] >> odd) & 1) && !f0;
     const int x2 = (D < e.maxd) && ((e.reach[D] >> (odd + 2)) & 1) && !f2;
-    uint32_t nt;
-    if (e.ordered) nt = ((uint32_t)(f0 | (x0 << 1)) << TD_CLASS_ZERO) | ((uint32_t)(f2 | (x2 << 1)) << TD_CLASS_PLUS2);
-    else nt = ((uint32_t)(f0 | (x0 << 2)) << TD_CLASS_ZERO) | ((uint32_t)(f2 | (x2 << 1)) << TD_CLASS_PLUS2);
+    uint32_t nt;  // byte c holds the flags of class c; byte 0 (filtered out) is zero
+    if (e.ordered) nt = ((uint32_t)(f0 | (x0 << 1)) << (8 * TD_CLASS_ZERO)) | ((uint32_t)(f2 | (x2 << 1)) << (8 * TD_CLASS_PLUS2));
+    else nt = ((uint32_t)(f0 | (x0 << 2)) << (8 * TD_CLASS_ZERO)) | ((uint32_t)(f2 | (x2 << 1)) << (8 * TD_CLASS_PLUS2));
     uint32_t fb[32];
     for (int lane = 0; lane < 32; ++lane) {
         fb[lane] = 0;
@@ -82,7 +82,7 @@ int evaluate(Emu &e, int level, int odd) {
             const int i = e.tri_i[t], j = e.tri_j[t], k = e.tri_k[t];
             const int idx = e.pt[i * TD_PT_STRIDE + j] | (e.pt[j * TD_PT_STRIDE + k] << 4) |
                             (e.pt[k * TD_PT_STRIDE + i] << 8);
-            const uint32_t tb = (nt >> e.lut[idx]) & 7u;
+            const uint32_t tb = (nt >> (8 * e.lut[idx])) & 7u;
             fb[lane] |= (tb & 1u) << s;
             e.m1[level][lane] |= ((tb >> 1) & 1u) << s;
             e.m2[level][lane] |= ((tb >> 2) & 1u) << s;

@@ -87,3 +87,13 @@ def test_device_symbol_replay_matches_oracle(td, oracle):
     want = [oracle.validate(b, o, abc, mm) is None for b, o, abc, mm in cases]
     assert got.tolist() == [int(w) for w in want]
     assert 0 < sum(want) < c
+
+
+@pytest.mark.gpu
+def test_emitter_shaped_run_replays_every_certificate(td, tmp_path):
+    from td16_b200 import emitter_run
+    out = str(tmp_path / "certs.bin")
+    r = emitter_run.run(count=20000, slots=4, budget=256 << 20, batch=4096, out_path=out, seed=4)
+    assert r["errors"] == 0 and r["found"] + r["not_found"] == 20000
+    assert r["certificates"] == r["found"] and r["replay"]["records"] == r["found"]
+    assert r["replay"]["accepted"] == r["replay"]["records"]

@@ -7,14 +7,16 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _requests(td, count, seed=3):
-    perms, n = td.synth_perms(seed, count, 8, 16, 0, 0, 0)
+def _requests(td, count, seed=3, n_max=16):
+    perms, n = td.synth_perms(seed, count, 8, n_max, 0, 0, 0)
     return td.prepare_perms(perms, n, (n // 2 + 1).astype(np.int32))
 
 
-@pytest.mark.parametrize("flags", [0, 1])
-def test_results_are_the_same_alone_and_in_the_mix(td, flags):
-    inst = _requests(td, 3000)
+# free order on the full request mix; the reference order (blind, so slow on
+# S_16) on n = 8..12
+@pytest.mark.parametrize("flags,n_max", [(0, 16), (1, 12)])
+def test_results_are_the_same_alone_and_in_the_mix(td, flags, n_max):
+    inst = _requests(td, 3000, n_max=n_max)
     # alone: each request by itself through a fresh launch, one at a time
     srv = td._lib.Server(0, 64, flags, 60.0)
     alone = []
