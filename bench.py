@@ -231,10 +231,11 @@ def run_engine(args):
             int(v) for v in replicas.sum_over_ranks([verified, expansions, found, not_found, errors], dist, dev)]
     value = verified / total_s
 
+    only_engine = args.legs == "engine"
     # end to end through the public host-buffer API
     host_in = inst.copy()
     e2e_s, e2e_verified = 0.0, 0
-    for k in range(max(1, min(args.steps, 3))):
+    for k in range(0 if only_engine else max(1, min(args.steps, 3))):
         t0 = time.perf_counter()
         res_h, st = td.search_batch(0, host_in, _lib.FLAG_VERIFY)
         e2e_s += time.perf_counter() - t0
@@ -242,15 +243,17 @@ def run_engine(args):
     e2e_steps = max(1, min(args.steps, 3))
 
     # the plain one-launch-per-batch form on the same GPU
-    pe = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-    with torch.cuda.stream(stream):
-        flush.zero_()
-    pe[0].record(stream)
-    step(_lib.FLAG_PLAIN)
-    pe[1].record(stream)
-    torch.cuda.synchronize()
-    plain_ms = pe[0].elapsed_time(pe[1])
-    plain_verified = int(d_ok.sum().item())
+    plain_ms, plain_verified = float("nan"), 0
+    if not only_engine:
+        pe = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        pe[0].record(stream)
+        step(_lib.FLAG_PLAIN)
+        pe[1].record(stream)
+        torch.cuda.synchronize()
+        plain_ms = pe[0].elapsed_time(pe[1])
+        plain_verified = int(d_ok.sum().item())
 
     if rank != 0:
         if dist:
@@ -279,7 +282,7 @@ def run_engine(args):
 
     graph.close()
     serving = None
-    if world == 1:
+    if world == 1 and not only_engine:
         perms_s, n_s = td.synth_perms(3, 100000, 8, 16, 0, 0, 0)
         inst_s = td.prepare_perms(perms_s, n_s, (n_s // 2 + 1).astype(np.int32))
         serving = {"workload": "open-loop Poisson, n uniform 8..16, bound floor(n/2)+1, 64 GiB frame pool"}
@@ -292,7 +295,7 @@ def run_engine(args):
                 serving[f"{int(rate)}_per_s"] = {"error": str(e)}
         _, bst = td.search_batch(0, inst_s, 0)
         serving["batched_per_s"] = len(inst_s) / (bst.kernel_ms / 1e3)
-    cpu = cpu_baseline() if world == 1 else None
+    cpu = cpu_baseline() if world == 1 and not only_engine else None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": mean_ms, "higher_is_better": True, "scaling": "weak",
@@ -302,7 +305,7 @@ def run_engine(args):
         "nodes_per_s": nodes_per_s, "triples_per_s": triples_per_s,
         "found": found, "not_found": not_found, "errors": errors, "verified": verified,
         "plain_one_launch": {"value": plain_verified / (plain_ms / 1e3), "ms": plain_ms},
-        "e2e": {"value": e2e_verified / e2e_s, "unit": UNIT, "h2d_bytes_per_step": count * 16,
+        "e2e": {"value": e2e_verified / e2e_s if e2e_s else None, "unit": UNIT, "h2d_bytes_per_step": count * 16,
                 "d2h_bytes_per_step": count * 32, "ms_per_step": e2e_s / e2e_steps * 1e3},
         "gpu_launches": args.steps * 3,
         "launch_shape": tuned,
@@ -322,6 +325,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--legs", default="all", choices=["all", "engine"],
+                    help="'engine' times only the device-resident batch (no e2e, plain, serving or CPU legs)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

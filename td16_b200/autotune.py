@@ -30,9 +30,9 @@ GRID = {
     "warps": [2, 4, 8],
     "grain": [1, 4, 16],
     "split_level": [2, 4, 6],
-    "check_every": [2, 8, 32],
+    "check_every": [8, 32, 128],
 }
-QUICK = {"warps": [4, 8], "grain": [4, 16], "split_level": [4], "check_every": [8]}
+QUICK = {"warps": [2, 4], "grain": [4, 8], "split_level": [4], "check_every": [32, 128]}
 
 
 def _configure(p):

@@ -274,6 +274,7 @@ TD_API long long td_cert_writer_enqueue_batch(void *handle, int count, const uin
         const td_result &r = results[i];
         if (r.status != TD_FOUND || r.depth <= 0 || r.depth > TD_CERT_MAX_MOVES) continue;
         const int N = n[i];
+        if (N < 3 || N > TD_CERT_MAX_N) return -1;
         uint8_t cur[TD_CERT_MAX_N], nxt[TD_CERT_MAX_N], abc[3 * TD_CERT_MAX_MOVES];
         std::memcpy(cur, beta + (size_t)i * TD_CERT_MAX_N, (size_t)N);
         for (int d = 0; d < r.depth; ++d) {  // GPUSortingSearch.java:229-238
@@ -344,6 +345,7 @@ TD_API long long td_cert_read_file(const char *path, int n, long long cap, uint8
 TD_API void td_pairs_from_perms(int count, const int8_t *perms, const uint8_t *n, uint8_t *beta, uint8_t *omega) {
     for (int i = 0; i < count; ++i) {
         int init;
+        if (n[i] > TD_CERT_MAX_N - 1) continue;
         td_perm_to_pair(perms + (size_t)i * 16, n[i], beta + (size_t)i * TD_CERT_MAX_N,
                         omega + (size_t)i * TD_CERT_MAX_N, &init);
     }

@@ -124,8 +124,12 @@ __global__ void __launch_bounds__(256) td_persistent_kernel(const td_instance *_
 // itself idle, and busy warps then hand the remaining children of their
 // shallowest DFS level to the item array.  Every wait is bounded by the
 // launch deadline; the launch ends when no ticket, item or unit is left.
-__device__ __forceinline__ void td_finish_unit(const td_dfs_out &r, td_inst_state *st, td_result *out,
-                                               const uint16_t *path) {
+// Ends one unit of a shared search: records a found witness (first finder
+// wins), and the unit that finishes the search last writes the final status
+// and the summed expansions.  Returns 1 in the warp that finished last.
+// System-scope fences: `out` may be host memory mapped into the device.
+__device__ __forceinline__ int td_finish_unit(const td_dfs_out &r, td_inst_state *st, td_result *out,
+                                              const uint16_t *path) {
     const int lane = threadIdx.x & 31;
     int win = 0, last = 0;
     if (lane == 0) {
@@ -137,9 +141,9 @@ __device__ __forceinline__ void td_finish_unit(const td_dfs_out &r, td_inst_stat
     if (win) td_write_result(out, TD_FOUND, r.depth, r.found_move, path, 0, 0, 7);
     __syncwarp();
     if (lane == 0) {
-        __threadfence();
+        __threadfence_system();
         last = atomicSub(&st->pending, 1) == 1;
-        if (last) __threadfence();
+        if (last) __threadfence_system();
     }
     last = __shfl_sync(TD_FULL, last, 0);
     if (last) {
@@ -155,7 +159,9 @@ __device__ __forceinline__ void td_finish_unit(const td_dfs_out &r, td_inst_stat
         exp = __shfl_sync(TD_FULL, exp, 0);
         if (!found) td_write_result(out, err ? err : TD_NOT_FOUND, 0, 0, path, exp, 0, 8);
         else td_write_result(out, TD_FOUND, 0, 0, path, exp, 7, 8);
+        __syncwarp();
     }
+    return last;
 }
 
 __global__ void __launch_bounds__(256) td_steal_kernel(const td_instance *__restrict__ in,
@@ -182,6 +188,8 @@ __global__ void __launch_bounds__(256) td_steal_kernel(const td_instance *__rest
     dc.grain = grain;
     dc.max_level = max_level;
     dc.check_every = check_every > 0 ? check_every : 1;
+    dc.ring = 0;
+    dc.deadline_ns = lim.deadline_ns;
     bool idle = false;
     unsigned backoff = 64;
     for (;;) {

@@ -311,10 +311,18 @@ struct td_pool {
     unsigned long long donated_items;
 };
 
+// Donated items live either in a per-launch array (batch launches: index i
+// at slot i, ready[i] == epoch once written) or in a ring (the serving launch:
+// index i at slot i % capacity, ready == td_ring_tag(i) once written and
+// td_ring_tag(i) | 0x80000000 once its taker has read it, which frees the slot).
+__device__ __forceinline__ uint32_t td_ring_tag(long long i) { return (uint32_t)((i + 1) & 0x7fffffff); }
+
 struct td_donate_ctx {
+    int ring;
+    uint64_t deadline_ns;   // bounds the wait for a ring slot to be freed
     td_pool *pool;
     td_item *items;
-    uint32_t *ready;        // ready[i] == epoch once item i is written
+    uint32_t *ready;
     uint32_t epoch;
     int capacity;
     int grain;              // at most this many items per donation
@@ -369,7 +377,10 @@ __device__ __forceinline__ int td_donate(td_warp_smem &s, const td_donate_ctx &d
     int base = -1;
     if (lane == 0) {
         int cur = *(volatile int *)&dc.pool->produced;
-        while (cur + give <= dc.capacity) {
+        for (;;) {
+            // a ring holds at most `capacity` items that are not yet claimed
+            const int used = dc.ring ? cur - *(volatile int *)&dc.pool->consumed : cur;
+            if (used + give > dc.capacity) break;
             const int prev = atomicCAS(&dc.pool->produced, cur, cur + give);
             if (prev == cur) { base = cur; break; }
             cur = prev;
@@ -407,9 +418,24 @@ __device__ __forceinline__ int td_donate(td_warp_smem &s, const td_donate_ctx &d
         it.off = (uint8_t)noff;
 #pragma unroll
         for (int d = 0; d < TD_MAX_DEPTH; ++d) it.path[d] = d < lv ? s.path[d] : (d == lv ? (uint16_t)t : 0);
-        dc.items[slot] = it;
+        int phys = slot;
+        uint32_t tag = dc.epoch;
+        if (dc.ring) {
+            phys = slot % dc.capacity;
+            tag = td_ring_tag(slot);
+            if (slot >= dc.capacity) {
+                // the slot's previous item (index slot - capacity) is claimed;
+                // wait until its taker has read it (bounded)
+                const uint32_t freed = td_ring_tag(slot - dc.capacity) | 0x80000000u;
+                for (unsigned spin = 0; *(volatile uint32_t *)&dc.ready[phys] != freed; ++spin) {
+                    if ((spin & 255u) == 0 && dc.deadline_ns && td_globaltimer() > dc.deadline_ns) break;
+                    __nanosleep(64);
+                }
+            }
+        }
+        dc.items[phys] = it;
         __threadfence();
-        atomicExch(&dc.ready[slot], dc.epoch);
+        atomicExch(&dc.ready[phys], tag);
         ++slot;
     }
     s.pm[lv][0][lane] = P0;

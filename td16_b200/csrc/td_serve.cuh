@@ -26,11 +26,18 @@ struct td_serve_dev_ctl {      // device memory: scheduler state of the launch
     unsigned long long served;
 };
 
+// Worker warps take fresh requests in arrival order and, in free order, also
+// donated subtrees of requests that others are searching (the batch engine's
+// donation scheme over a ring of items), so one hard request does not hold a
+// single warp for its whole search.  The warp that finishes a request last
+// writes its result and stamps done[slot] = request + 1.
 template <bool ORDERED>
 __global__ void __launch_bounds__(256) td_serve_kernel(const td_instance *ring, td_result *results,
                                                       volatile unsigned long long *done, unsigned ring_size,
                                                       td_serve_host_ctl *hctl, td_serve_dev_ctl *dctl,
-                                                      td_instance *queue, uint64_t max_exp,
+                                                      td_instance *queue, td_inst_state *state, td_pool *pool,
+                                                      td_item *items, uint32_t *ready, int item_capacity,
+                                                      int grain, int max_level, int check_every, uint64_t max_exp,
                                                       uint64_t time_limit_ns) {
     extern __shared__ __align__(16) uint8_t td_smem[];
     const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -80,52 +87,163 @@ __global__ void __launch_bounds__(256) td_serve_kernel(const td_instance *ring, 
     lim.max_expansions = max_exp ? max_exp : ~0ull;
     lim.deadline_ns = deadline;
     lim.abort_flag = nullptr;
+    td_donate_ctx dc;
+    dc.ring = 1;
+    dc.deadline_ns = deadline;
+    dc.pool = pool;
+    dc.items = items;
+    dc.ready = ready;
+    dc.epoch = 0;
+    dc.capacity = item_capacity;
+    dc.grain = grain;
+    dc.max_level = max_level;
+    dc.check_every = check_every > 0 ? check_every : 1;
+    bool idle = false;
     unsigned backoff = 128;
     for (;;) {
-        long long r = -1;
-        int stop = 0;
+        int kind = 0;
+        long long unit = -1;
         if (lane == 0) {
             const unsigned long long av = *(volatile unsigned long long *)&dctl->available;
             unsigned long long c = *(volatile unsigned long long *)&dctl->claimed;
             while (c < av) {
                 const unsigned long long prev = atomicCAS(&dctl->claimed, c, c + 1);
-                if (prev == c) { r = (long long)c; break; }
+                if (prev == c) { kind = 1; unit = (long long)c; break; }
                 c = prev;
             }
-            if (r < 0) {
+            if (!kind && !ORDERED) {
+                const int P = *(volatile int *)&pool->produced;
+                int C = *(volatile int *)&pool->consumed;
+                while (C < P) {
+                    const int prev = atomicCAS(&pool->consumed, C, C + 1);
+                    if (prev == C) { kind = 2; unit = C; break; }
+                    C = prev;
+                }
+            }
+            if (kind) atomicAdd(&pool->active, 1);  // counts holders only
+        }
+        kind = __shfl_sync(TD_FULL, kind, 0);
+        unit = __shfl_sync(TD_FULL, unit, 0);
+        if (!kind) {
+            int stop = 0;
+            if (lane == 0) {
                 stop = *(volatile int *)&dctl->stop;
-                if (stop) {  // drain: the dispatcher publishes before it stops
+                if (stop) {  // drain: every published request claimed and no unit left
                     const unsigned long long av2 = *(volatile unsigned long long *)&dctl->available;
                     const unsigned long long c2 = *(volatile unsigned long long *)&dctl->claimed;
-                    stop = c2 >= av2;
+                    stop = c2 >= av2 && *(volatile int *)&pool->active == 0 &&
+                           *(volatile int *)&pool->consumed >= *(volatile int *)&pool->produced;
                 }
                 if (td_globaltimer() > deadline) stop = 1;
+                if (!stop && !idle) { atomicAdd(&pool->idle, 1); idle = true; }
             }
-            __threadfence();
-        }
-        r = __shfl_sync(TD_FULL, r, 0);
-        if (r < 0) {
             if (__shfl_sync(TD_FULL, stop, 0)) break;
             __nanosleep(backoff);
-            backoff = min(backoff * 2u, 1024u);
+            backoff = min(backoff * 2u, 2048u);
             continue;
         }
+        if (lane == 0 && idle) { atomicSub(&pool->idle, 1); idle = false; }
         backoff = 128;
-        const unsigned slot = (unsigned)(r % ring_size);
-        td_instance x;
-        {
+        long long req = unit;
+        td_dfs_out r;
+        r.status = TD_DFS_ABORTED;
+        r.depth = 0;
+        r.found_move = 0;
+        r.expansions = 0;
+        bool run = false;
+        int d0 = 0;
+        if (kind == 1) {
+            const unsigned slot = (unsigned)(req % ring_size);
             const uint4 v = __ldcg(reinterpret_cast<const uint4 *>(&queue[slot]));
-            x = *reinterpret_cast<const td_instance *>(&v);
+            const td_instance x = *reinterpret_cast<const td_instance *>(&v);
+            td_inst_state *st = &state[slot];
+            if (lane == 0) {  // the slot's previous request is done: start afresh
+                st->found = 0;
+                st->expansions = 0;
+                st->error = 0;
+                st->pending = 1;
+                __threadfence();
+            }
+            __syncwarp();
+            if (!td_instance_ok(x) || td_triple_count(x.n_symbols) == 0) {
+                td_write_result(&results[slot], td_instance_ok(x) ? TD_NOT_FOUND : TD_ERR_ARG, 0, 0, s.path, 0,
+                                0, 8);
+                __threadfence_system();
+                __syncwarp();
+                if (lane == 0) {
+                    done[slot] = (unsigned long long)req + 1ull;
+                    atomicAdd(&dctl->served, 1ull);
+                }
+            } else {
+                td_setup_root(s, x, code, codeN);
+                run = true;
+            }
+        } else {
+            // a donated subtree: wait until it is written, copy it, free the slot
+            const int phys = (int)(unit % item_capacity);
+            const uint32_t tag = td_ring_tag(unit);
+            int ok = 0;
+            if (lane == 0) {
+                for (unsigned spin = 0; spin < (1u << 30); ++spin) {
+                    if (*(volatile uint32_t *)&ready[phys] == tag) { ok = 1; break; }
+                    if ((spin & 1023u) == 0 && td_globaltimer() > deadline) break;
+                    __nanosleep(32);
+                }
+                if (!ok) atomicCAS(&dctl->error, 0, TD_ERR_TIMEOUT);
+                __threadfence();
+            }
+            ok = __shfl_sync(TD_FULL, ok, 0);
+            if (ok) {
+                td_item it;
+                {
+                    const uint4 *src = reinterpret_cast<const uint4 *>(&items[phys]);
+                    uint4 *dst = reinterpret_cast<uint4 *>(&it);
+                    dst[0] = __ldcg(src);
+                    dst[1] = __ldcg(src + 1);
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    __threadfence();
+                    atomicExch(&ready[phys], tag | 0x80000000u);
+                }
+                req = it.inst;
+                const unsigned slot = (unsigned)(req % ring_size);
+                const uint4 v = __ldcg(reinterpret_cast<const uint4 *>(&queue[slot]));
+                const td_instance x = *reinterpret_cast<const td_instance *>(&v);
+                td_setup_root(s, x, code, codeN);
+                d0 = it.depth;
+                if (lane == 0) {
+                    s.L[d0] = it.L;
+                    s.off[d0] = it.off;
+                    for (int d = 0; d < d0; ++d) s.path[d] = it.path[d];
+                }
+                __syncwarp();
+                int stop = 0;
+                if (lane == 0) stop = *(volatile int *)&state[slot].found;
+                run = !__shfl_sync(TD_FULL, stop, 0);
+                if (!run) {  // the request already has its witness
+                    if (td_finish_unit(r, &state[slot], &results[slot], s.path) && lane == 0) {
+                        done[slot] = (unsigned long long)req + 1ull;
+                        atomicAdd(&dctl->served, 1ull);
+                    }
+                }
+            }
         }
-        td_result *res = &results[slot];
-        td_warp_search<ORDERED>(x, res, s, lut, code, codeN, lim);
-        __threadfence_system();
-        __syncwarp();
-        if (lane == 0) {
-            done[slot] = (unsigned long long)r + 1ull;
-            atomicAdd(&dctl->served, 1ull);
+        if (run) {
+            const unsigned slot = (unsigned)(req % ring_size);
+            const uint4 v = __ldcg(reinterpret_cast<const uint4 *>(&queue[slot]));
+            const td_instance x = *reinterpret_cast<const td_instance *>(&v);
+            dc.inst = (uint32_t)req;
+            dc.state = &state[slot];
+            r = td_dfs<ORDERED>(s, lut, code, x.n_symbols, x.max_moves, d0, lim, ORDERED ? nullptr : &dc);
+            if (td_finish_unit(r, &state[slot], &results[slot], s.path) && lane == 0) {
+                done[slot] = (unsigned long long)req + 1ull;
+                atomicAdd(&dctl->served, 1ull);
+            }
         }
+        if (lane == 0) atomicSub(&pool->active, 1);
     }
+    if (lane == 0 && idle) atomicSub(&pool->idle, 1);
 }
 
 // ============================================================================
@@ -145,6 +263,11 @@ struct Server {
     td_serve_host_ctl *h_ctl = nullptr, *d_hctl = nullptr;
     td_serve_dev_ctl *d_ctl = nullptr;
     td_instance *d_queue = nullptr;
+    td_inst_state *d_state = nullptr;
+    td_pool *d_pool = nullptr;
+    td_item *d_items = nullptr;
+    uint32_t *d_ready = nullptr;
+    int item_capacity = 0;
     unsigned long long published = 0;
     int workers = 0;
 };
@@ -159,6 +282,10 @@ void server_free(Server *sv) {
     if (sv->h_ctl) cudaFreeHost(sv->h_ctl);
     if (sv->d_ctl) cudaFree(sv->d_ctl);
     if (sv->d_queue) cudaFree(sv->d_queue);
+    if (sv->d_state) cudaFree(sv->d_state);
+    if (sv->d_pool) cudaFree(sv->d_pool);
+    if (sv->d_items) cudaFree(sv->d_items);
+    if (sv->d_ready) cudaFree(sv->d_ready);
     if (sv->stream) cudaStreamDestroy(sv->stream);
     delete sv;
 }
@@ -205,6 +332,15 @@ TD_API int td_serve_open(int device, unsigned ring_size, unsigned flags, double 
     if ((e = cudaMalloc(&sv->d_ctl, sizeof(td_serve_dev_ctl))) != cudaSuccess) return fail(e, __LINE__);
     if ((e = cudaMalloc(&sv->d_queue, sizeof(td_instance) * ring_size)) != cudaSuccess) return fail(e, __LINE__);
     if ((e = cudaMemsetAsync(sv->d_ctl, 0, sizeof(td_serve_dev_ctl), sv->stream)) != cudaSuccess) return fail(e, __LINE__);
+    // donation ring: 64 items per ring slot of requests, at least 2^16
+    sv->item_capacity = (int)std::min<size_t>(1u << 24, std::max<size_t>(1u << 16, (size_t)ring_size * 64));
+    if ((e = cudaMalloc(&sv->d_state, sizeof(td_inst_state) * ring_size)) != cudaSuccess) return fail(e, __LINE__);
+    if ((e = cudaMalloc(&sv->d_pool, sizeof(td_pool))) != cudaSuccess) return fail(e, __LINE__);
+    if ((e = cudaMalloc(&sv->d_items, sizeof(td_item) * sv->item_capacity)) != cudaSuccess) return fail(e, __LINE__);
+    if ((e = cudaMalloc(&sv->d_ready, sizeof(uint32_t) * sv->item_capacity)) != cudaSuccess) return fail(e, __LINE__);
+    if ((e = cudaMemsetAsync(sv->d_pool, 0, sizeof(td_pool), sv->stream)) != cudaSuccess) return fail(e, __LINE__);
+    if ((e = cudaMemsetAsync(sv->d_ready, 0, sizeof(uint32_t) * sv->item_capacity, sv->stream)) != cudaSuccess)
+        return fail(e, __LINE__);
     const int warps = g_warps_per_block;
     const size_t smem = smem_bytes(warps);
     int per_sm = 0;
@@ -220,11 +356,15 @@ TD_API int td_serve_open(int device, unsigned ring_size, unsigned flags, double 
     sv->workers = grid * warps - 1;
     const uint64_t limit_ns = (uint64_t)((time_limit_s > 0 ? time_limit_s : 60.0) * 1e9);
     if (ordered)
-        td_serve_kernel<true><<<grid, warps * 32, smem, sv->stream>>>(sv->d_ring, sv->d_res, sv->d_done, ring_size,
-                                                                      sv->d_hctl, sv->d_ctl, sv->d_queue, 0, limit_ns);
+        td_serve_kernel<true><<<grid, warps * 32, smem, sv->stream>>>(
+            sv->d_ring, sv->d_res, sv->d_done, ring_size, sv->d_hctl, sv->d_ctl, sv->d_queue, sv->d_state,
+            sv->d_pool, sv->d_items, sv->d_ready, sv->item_capacity, g_steal_grain, g_split_level, g_check_every, 0,
+            limit_ns);
     else
-        td_serve_kernel<false><<<grid, warps * 32, smem, sv->stream>>>(sv->d_ring, sv->d_res, sv->d_done, ring_size,
-                                                                       sv->d_hctl, sv->d_ctl, sv->d_queue, 0, limit_ns);
+        td_serve_kernel<false><<<grid, warps * 32, smem, sv->stream>>>(
+            sv->d_ring, sv->d_res, sv->d_done, ring_size, sv->d_hctl, sv->d_ctl, sv->d_queue, sv->d_state,
+            sv->d_pool, sv->d_items, sv->d_ready, sv->item_capacity, g_steal_grain, g_split_level, g_check_every, 0,
+            limit_ns);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, __LINE__);
     *handle = sv;
     return TD_OK;

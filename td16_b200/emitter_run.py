@@ -93,8 +93,9 @@ def run(count: int, slots: int, budget: int, batch: int, out_path: str, seed: in
                 inst = _lib.prepare_perms(perms, n, 9)
                 beta, omega = _pairs(perms, n)
                 res, st = _lib.search_batch(slot, inst, _lib.FLAG_VERIFY)
+                symbols = (n + 1).astype(np.uint8)  # held: ctypes only keeps its address
                 q = _lib.lib().td_cert_writer_enqueue_batch(writer._h, c, _lib._ptr(beta), _lib._ptr(omega),
-                                                            _lib._ptr((n + 1).astype(np.uint8)), _lib._ptr(res))
+                                                            _lib._ptr(symbols), _lib._ptr(res))
                 if q < 0:
                     raise _lib.TdError(_lib.CUDA_ERROR, "certificate sink rejected a batch")
                 with lock:
