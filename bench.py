@@ -103,9 +103,16 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def make_instances(td, rank):
+def make_instances(td, rank, count=COUNT, workload="mix"):
     from td16_b200.replicas import rank_seed
-    perms, n = td.synth_perms(rank_seed(SEED, rank), COUNT, 16, 16, 50, 1, 4)
+    if workload == "replicated":
+        # one near-reverse S_16 instance (seed 2, index 0: 895 expansions in
+        # free order) copied `count` times: every warp works for the whole
+        # launch, so counters describe the search itself, not a tail
+        perms, n = td.synth_perms(SEED, 1, 16, 16, 100, 1, 4)
+        perms, n = np.repeat(perms, count, axis=0), np.repeat(n, count)
+        return td.prepare_perms(perms, n, MAX_MOVES), perms, n
+    perms, n = td.synth_perms(rank_seed(SEED, rank), count, 16, 16, 50, 1, 4)
     return td.prepare_perms(perms, n, MAX_MOVES), perms, n
 
 
@@ -179,7 +186,7 @@ def run_engine(args):
     stream_ptr = _lib.lib().td_slot_stream(0)
     stream = torch.cuda.ExternalStream(stream_ptr, device=dev)
 
-    inst, perms, n = make_instances(td, rank)
+    inst, perms, n = make_instances(td, rank, args.count, args.workload)
     count = len(inst)
     d_in = torch.from_numpy(inst.view(np.uint8).copy()).to(dev)
     d_out = torch.zeros(count * 32, dtype=torch.uint8, device=dev)
@@ -325,6 +332,10 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--count", type=int, default=COUNT,
+                    help="instances per GPU (default 2^20, the benchmark workload; smaller for profiling)")
+    ap.add_argument("--workload", default="mix", choices=["mix", "replicated"],
+                    help="'replicated': one hard instance copied, for profiling the search without a tail")
     ap.add_argument("--legs", default="all", choices=["all", "engine"],
                     help="'engine' times only the device-resident batch (no e2e, plain, serving or CPU legs)")
     args = ap.parse_args()
