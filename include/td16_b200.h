@@ -160,6 +160,22 @@ int td_search_batch_device(int slot, int count, const td_instance *d_instances,
                            uint64_t max_expansions, void *stream, char *err,
                            size_t errlen);
 
+/* Batch search that allocates no device memory (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc/cudaFree: a slot worker
+ * that must not stall on the device-wide synchronisation those calls can
+ * imply while other searches run, or a process whose device memory is held by
+ * another allocator.  The caller passes device buffers for instances and
+ * results; all scratch is a fixed 3.25 MiB static device array per GPU, kept
+ * until the process exits.  Runs on the calling thread's current device and
+ * enqueues on `stream`.  At most 65536 instances per call (more returns
+ * TD_INVALID_ARG).  The first call on a device does a one-time set-up (table
+ * uploads and an address query), so make it before any stream capture.  Calls
+ * share the scratch: launches that overlap on the GPU race, so serialise them. */
+int td_search_batch_noalloc(int count, const td_instance *d_instances,
+                            td_result *d_results, unsigned flags,
+                            uint64_t max_expansions, void *stream, char *err,
+                            size_t errlen);
+
 /* CUDA-graph form of a batch over fixed device buffers: capture once, replay
  * with one graph launch per batch (scratch epochs advance on the device). */
 int td_batch_graph_create(int slot, int count, const td_instance *d_instances,

@@ -1042,6 +1042,166 @@ TD_API int td_int_issue_peak(int device, float target_ms, double *warp_inst_per_
     return TD_OK;
 }
 
+// ---- batch search without device allocation ----------------------------------
+//
+// td_search_batch_noalloc is for callers that cannot call cudaMalloc or
+// cudaFree: a slot worker that must not stall on the device-wide
+// synchronisation those calls can imply while other slots' searches run on
+// their own streams, or a host process whose device memory is already held by
+// another allocator, so that a new allocation would fail although the caller's
+// buffers exist.  The caller passes device buffers for instances and results;
+// every other byte the search needs lives in td_noalloc_scratch below, a
+// fixed array that each GPU loading this library holds until the process
+// exits.  Limits: TD_NOALLOC_MAX_INSTANCES instances per call and
+// TD_NOALLOC_ITEMS donated subtrees in flight (when the item space is full the
+// donor keeps the work, so a full item space only costs balance, not results).
+// All calls share this one array and it keeps the last call's contents, so
+// calls whose launches overlap on the GPU race with each other: serialise
+// them (e.g. issue them on one stream).
+
+#define TD_NOALLOC_MAX_INSTANCES 65536
+#define TD_NOALLOC_ITEMS 65536
+#define TD_NOALLOC_HEAD 256                                             // pool, epoch, ticket
+#define TD_NOALLOC_STATE_OFF TD_NOALLOC_HEAD
+#define TD_NOALLOC_ITEMS_OFF (TD_NOALLOC_STATE_OFF + TD_NOALLOC_MAX_INSTANCES * 16)
+#define TD_NOALLOC_READY_OFF (TD_NOALLOC_ITEMS_OFF + TD_NOALLOC_ITEMS * 32)
+#define TD_NOALLOC_BYTES (TD_NOALLOC_READY_OFF + TD_NOALLOC_ITEMS * 4)   // 3.25 MiB + 256 B
+
+static_assert(sizeof(td_pool) + 2 * sizeof(uint32_t) <= TD_NOALLOC_HEAD, "scratch head");
+static_assert(sizeof(td_inst_state) == 16 && sizeof(td_item) == 32, "scratch records");
+
+static __device__ __align__(256) uint8_t td_noalloc_scratch[TD_NOALLOC_BYTES];
+
+namespace {
+
+constexpr int kNoAllocDevices = 64;
+
+// error reporting without heap use
+#define TD_CHECK_NA(call)                                                                          \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) {                                                                   \
+            if (err && errlen)                                                                     \
+                std::snprintf(err, errlen, "%s:%d: CUDA error %s (%s)", __FILE__, __LINE__,         \
+                              cudaGetErrorName(e_), cudaGetErrorString(e_));                       \
+            return TD_CUDA_ERROR;                                                                  \
+        }                                                                                          \
+    } while (0)
+#define TD_FAIL_NA(...)                                            \
+    do {                                                           \
+        if (err && errlen) std::snprintf(err, errlen, __VA_ARGS__); \
+        return TD_INVALID_ARG;                                     \
+    } while (0)
+
+struct NoAllocDevice {
+    bool ready;
+    uint8_t *scratch;  // device address of td_noalloc_scratch on this device
+    int sms;
+    int steal_blocks;
+    int persistent_blocks;
+};
+
+std::mutex g_noalloc_mu;
+NoAllocDevice g_noalloc[kNoAllocDevices];
+uint16_t g_noalloc_tri[TD_TRI_TABLE];  // host copies of the device tables, no heap
+uint8_t g_noalloc_lut[TD_LUT_BYTES];
+
+// Once per device, with that device current: uploads the triple and class
+// tables and takes the scratch array's device address.  In host code the
+// name td_noalloc_scratch is only a host-side stand-in, never a device address.
+int noalloc_setup(int device, char *err, size_t errlen) {
+    NoAllocDevice &d = g_noalloc[device];
+    if (d.ready) return TD_OK;
+    for (int N = 3; N <= TD_MAX_N; ++N) {
+        int t = 0;
+        const int base = td_tri_base(N);
+        for (int i = 0; i < N - 2; ++i)
+            for (int j = i + 1; j < N - 1; ++j)
+                for (int k = j + 1; k < N; ++k) g_noalloc_tri[base + t++] = td_pack_move(i, j, k);
+    }
+    for (int i = 0; i < TD_LUT_BYTES; ++i) g_noalloc_lut[i] = (uint8_t)td_class_of_index(i);
+    TD_CHECK_NA(cudaMemcpyToSymbol(td_tri_table, g_noalloc_tri, sizeof g_noalloc_tri));
+    TD_CHECK_NA(cudaMemcpyToSymbol(td_lut_global, g_noalloc_lut, sizeof g_noalloc_lut));
+    void *ptr = nullptr;
+    TD_CHECK_NA(cudaGetSymbolAddress(&ptr, td_noalloc_scratch));
+    TD_CHECK_NA(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device));
+    const size_t smem = smem_bytes(4);
+    TD_CHECK_NA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.steal_blocks, td_steal_kernel, 128, smem));
+    TD_CHECK_NA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.persistent_blocks, td_persistent_kernel<true>,
+                                                              128, smem));
+    d.scratch = static_cast<uint8_t *>(ptr);
+    d.ready = true;
+    return TD_OK;
+}
+
+}  // namespace
+
+// Batch search on the calling thread's current device that allocates no
+// device memory.  d_instances / d_results: caller-owned device buffers of
+// `count` records; flags as for td_search_batch_device (TD_FLAG_ORDERED,
+// TD_FLAG_PLAIN, TD_FLAG_VERIFY).  Enqueues on `stream` and returns.  The
+// first call on a device performs the one-time set-up above (table uploads
+// and a symbol-address query, both synchronous), so make that first call
+// before any stream capture.  count > 65536 is rejected.
+TD_API int td_search_batch_noalloc(int count, const td_instance *d_instances, td_result *d_results, unsigned flags,
+                                   uint64_t max_exp, void *stream, char *err, size_t errlen) {
+    if (count < 0 || count > TD_NOALLOC_MAX_INSTANCES)
+        TD_FAIL_NA("td_search_batch_noalloc: count %d outside 0..%d (the fixed scratch holds at most %d instances)",
+                   count, TD_NOALLOC_MAX_INSTANCES, TD_NOALLOC_MAX_INSTANCES);
+    if (count == 0) return TD_OK;
+    if (!d_instances || !d_results) TD_FAIL_NA("td_search_batch_noalloc: null instance or result buffer");
+    int device = 0;
+    TD_CHECK_NA(cudaGetDevice(&device));
+    if (device < 0 || device >= kNoAllocDevices)
+        TD_FAIL_NA("td_search_batch_noalloc: device ordinal %d out of range", device);
+    NoAllocDevice d;
+    {
+        std::lock_guard<std::mutex> g(g_noalloc_mu);
+        const int rc = noalloc_setup(device, err, errlen);
+        if (rc != TD_OK) return rc;
+        d = g_noalloc[device];
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const int warps = 4, threads = 128;
+    const size_t smem = smem_bytes(warps);
+    const bool ordered = flags & TD_FLAG_ORDERED;
+    const uint64_t limit = time_limit_ns();
+    td_pool *pool = reinterpret_cast<td_pool *>(d.scratch);
+    uint32_t *epoch = reinterpret_cast<uint32_t *>(d.scratch + sizeof(td_pool));
+    int *ticket = reinterpret_cast<int *>(d.scratch + sizeof(td_pool) + sizeof(uint32_t));
+    td_inst_state *state = reinterpret_cast<td_inst_state *>(d.scratch + TD_NOALLOC_STATE_OFF);
+    td_item *items = reinterpret_cast<td_item *>(d.scratch + TD_NOALLOC_ITEMS_OFF);
+    uint32_t *ready = reinterpret_cast<uint32_t *>(d.scratch + TD_NOALLOC_READY_OFF);
+    const int blocks_needed = (count + warps - 1) / warps;
+    if (flags & TD_FLAG_PLAIN) {
+        if (ordered)
+            td_plain_kernel<true><<<blocks_needed, threads, smem, st>>>(d_instances, d_results, count, max_exp, limit);
+        else
+            td_plain_kernel<false><<<blocks_needed, threads, smem, st>>>(d_instances, d_results, count, max_exp, limit);
+    } else if (ordered) {
+        TD_CHECK_NA(cudaMemsetAsync(ticket, 0, sizeof(int), st));
+        const int grid = std::max(1, std::min(d.sms * std::max(1, d.persistent_blocks), blocks_needed));
+        td_persistent_kernel<true><<<grid, threads, smem, st>>>(d_instances, d_results, count, ticket, 1, max_exp,
+                                                                limit);
+    } else {
+        // counters and per-instance state start at zero on every call; items
+        // are tagged with a fresh epoch so an earlier call's items never count
+        TD_CHECK_NA(cudaMemsetAsync(pool, 0, sizeof(td_pool), st));
+        TD_CHECK_NA(cudaMemsetAsync(state, 0, (size_t)count * sizeof(td_inst_state), st));
+        td_epoch_kernel<<<1, 1, 0, st>>>(epoch);
+        const int grid = std::max(1, std::min(d.sms * std::max(1, d.steal_blocks), blocks_needed));
+        td_steal_kernel<<<grid, threads, smem, st>>>(d_instances, d_results, count, pool, items, ready, epoch,
+                                                     TD_NOALLOC_ITEMS, state, g_steal_grain, g_split_level,
+                                                     g_check_every, limit);
+    }
+    TD_CHECK_NA(cudaGetLastError());
+    if (flags & TD_FLAG_VERIFY) {
+        td_validate_kernel<<<(count + 255) / 256, 256, 0, st>>>(d_instances, d_results, nullptr, count, 1);
+        TD_CHECK_NA(cudaGetLastError());
+    }
+    return TD_OK;
+}
+
 // ---- CUDA graphs -------------------------------------------------------------
 
 namespace {
