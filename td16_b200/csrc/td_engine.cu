@@ -392,6 +392,7 @@ struct Slot {
     td_inst_state *d_state = nullptr;
     size_t state_count = 0;
     uint32_t *d_epoch = nullptr;
+    int slots_on_device = 1;
     std::mutex *mu = nullptr;
 };
 
@@ -541,7 +542,11 @@ int launch_batch(Slot &s, int count, const td_instance *d_in, td_result *d_out, 
             TD_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, td_steal_kernel, threads, smem));
             d.steal_blocks_per_sm = std::max(1, b);
         }
-        const int grid = std::max(1, std::min(d.sms * d.steal_blocks_per_sm, (count + warps - 1) / warps));
+        // at least the slot's share of the resident grid, so that a small batch
+        // (one search from td_search) is spread over that many warps by donation
+        const int resident = d.sms * d.steal_blocks_per_sm;
+        const int share = std::max(1, resident / std::max(1, s.slots_on_device));
+        const int grid = std::max(1, std::min(resident, std::max(share, (count + warps - 1) / warps)));
         TD_CHECK(cudaMemsetAsync(s.d_pool, 0, sizeof(td_pool), stream));
         TD_CHECK(cudaMemsetAsync(s.d_state, 0, (size_t)count * sizeof(td_inst_state), stream));
         td_epoch_kernel<<<1, 1, 0, stream>>>(s.d_epoch);
@@ -611,7 +616,11 @@ int search_one(int slot, const uint8_t *beta, const uint8_t *omega, int n, int i
     TD_CHECK(cudaSetDevice(s->device));
     *s->h_inst = x;
     TD_CHECK(cudaMemcpyAsync(s->d_inst, s->h_inst, sizeof(td_instance), cudaMemcpyHostToDevice, s->stream));
-    int rc = launch_batch(*s, 1, s->d_inst, s->d_res, flags | TD_FLAG_PLAIN, 0, s->stream, err, errlen);
+    // free order: the donation engine over the slot's share of the GPU (as the
+    // reference gives each slot SMs x resident blocks / slots queues,
+    // sorting_search.cu:740-752); the reference order keeps one warp
+    const unsigned how = (flags & TD_FLAG_ORDERED) ? (flags | TD_FLAG_PLAIN) : flags;
+    int rc = launch_batch(*s, 1, s->d_inst, s->d_res, how, 0, s->stream, err, errlen);
     if (rc != TD_OK) return rc;
     TD_CHECK(cudaMemcpyAsync(s->h_res, s->d_res, sizeof(td_result), cudaMemcpyDeviceToHost, s->stream));
     TD_CHECK(cudaEventRecord(s->done, s->stream));
@@ -745,6 +754,7 @@ TD_API int td_init_slots(int total_slots, const int *devices, int device_count, 
         Slot &s = g_slots[i];
         s.device = devices[i % device_count];
         s.budget = budget;
+        s.slots_on_device = per[s.device];
         s.mu = new std::mutex();
         cudaError_t e = cudaSetDevice(s.device);
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
