@@ -42,7 +42,8 @@ def replay_file(path: str, n_symbols: int, chunk: int = 1 << 20) -> dict:
     import torch
     total, accepted = 0, 0
     t0 = time.perf_counter()
-    cap = max(1, os.path.getsize(path) // 4)
+    # a record holds 2 length bytes, the key and a value of at least 2 bytes
+    cap = max(1, os.path.getsize(path) // (2 + (5 * n_symbols + 7) // 8 + 2))
     omega = np.zeros((cap, 17), np.uint8)
     abc = np.zeros((cap, 27), np.uint8)
     depth = np.zeros(cap, np.uint8)
