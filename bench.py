@@ -38,10 +38,16 @@ MAX_MOVES = 9
 METRIC = "verified witnesses/s (S_16, d<=9)"
 UNIT = "witnesses/s"
 WORKLOAD = "full-size decision search: 2^20 S_16 perms, 50% uniform / 50% reverse o 1-4 transpositions, d<=9"
-# warp instructions executed per node expansion by the search kernel at N=17,
-# from the ncu capture summarised in profiles/td_persistent_kernel_s16.md
-INST_PER_EXPANSION = None
-
+# Per node expansion at N = 17, the search kernel's warp instructions (all
+# pipes) and those of the integer ALU pipe, and its DRAM bytes per launch:
+# ncu capture of td_steal_kernel on 65,536 copies of one S_16 instance (tuned
+# launch shape), summarised in profiles/td_steal_kernel_s16_replicated_64k.md:
+# 36.611 G warp instructions over 61.897 M expansions; the ALU pipe busy
+# 84.886% of 2 warp instructions per cycle over 13.539 G SM cycles; 2.24 MB of
+# DRAM traffic.
+INST_PER_EXPANSION = 36.611e9 / 61.897e6
+ALU_INST_PER_EXPANSION = 0.84886 * 2 * 13.539e9 / 61.897e6
+DRAM_BYTES_PER_64K_LAUNCH = 2.24e6
 
 def rank_info():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
@@ -267,25 +273,32 @@ def run_engine(args):
             dist.destroy_process_group()
         return
 
-    # roofline: integer issue of the search kernel against the measured ALU peak
+    # roofline: instruction issue of the search kernel against the measured issue peak
     import ctypes as C
-    peak, pk_ms = C.c_double(), C.c_double()
+    issue_peak, alu_peak = C.c_double(), C.c_double()
     err = C.create_string_buffer(256)
     _lib.lib().td_int_issue_peak.argtypes = [C.c_int, C.c_float, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                              C.c_char_p, C.c_size_t]
-    _lib.lib().td_int_issue_peak(local, 200.0, C.byref(peak), C.byref(pk_ms), err, 256)
+    _lib.check(_lib.lib().td_int_issue_peak(local, 200.0, C.byref(issue_peak), C.byref(alu_peak), err, 256), err)
     per_step_exp = expansions / max(1, args.steps) / world
     mean_ms = float(np.mean(step_ms))
     nodes_per_s = per_step_exp / (mean_ms / 1e3)
     triples_per_s = nodes_per_s * 680
-    roofline = {"bound": "int-issue", "unit": "Gwarp-inst/s", "peak": peak.value / 1e9,
-                "peak_source": "measured live: LOP3 chains on every SM (td_int_issue_peak)",
-                "achieved": None, "frac": None, "traffic": None,
+    # The bound is the integer ALU pipe (LOP3/shift/compare work of the
+    # bit-sliced classification).  achieved: the search's ALU instructions per
+    # second (expansions/s x ALU instructions per expansion); peak: LOP3 chains
+    # on every SM, measured live.  Issue of all pipes is reported beside it.
+    ach = nodes_per_s * ALU_INST_PER_EXPANSION
+    roofline = {"bound": "int-alu", "unit": "G warp-inst/s", "achieved": ach / 1e9, "peak": alu_peak.value / 1e9,
+                "frac": ach / alu_peak.value,
+                "peak_source": "measured live: LOP3 chains on every SM (td_int_issue_peak), of measured",
+                "alu_inst_per_expansion": ALU_INST_PER_EXPANSION,
+                "issue_achieved": nodes_per_s * INST_PER_EXPANSION / 1e9,
+                "issue_peak_lop3_imad": issue_peak.value / 1e9,
+                "inst_per_expansion": INST_PER_EXPANSION,
+                "traffic": DRAM_BYTES_PER_64K_LAUNCH * count / 65536,
+                "traffic_note": "DRAM bytes per launch, ncu on 65,536 instances scaled by instance count",
                 "nodes_per_s": nodes_per_s, "triples_per_s": triples_per_s}
-    if INST_PER_EXPANSION:
-        ach = nodes_per_s * INST_PER_EXPANSION
-        roofline["achieved"] = ach / 1e9
-        roofline["frac"] = ach / peak.value
 
     graph.close()
     serving = None

@@ -121,6 +121,9 @@ int td_set_time_limit(double seconds);
 /* Work donation of the free-order engine: items per donation, deepest level
  * whose children may be donated, expansions between idle checks. */
 int td_configure_steal(int grain, int split_level, int check_every);
+/* The same for later serving launches (td_serve_open), kept apart because a
+ * serving launch trades throughput for latency (default 1, 2, 32). */
+int td_configure_serve(int grain, int split_level, int check_every);
 
 /* ---- instance preparation (host, no GPU needed) -------------------------- */
 
@@ -192,11 +195,13 @@ int td_validate_batch_device(int count, const td_instance *d_instances,
                              const td_result *d_results, uint8_t *d_ok,
                              void *stream, char *err, size_t errlen);
 
-/* Measures the device's ALU-pipe integer issue rate (warp instructions per
- * second of independent LOP3 chains at full occupancy), the denominator of the
- * search kernel's roofline. */
-int td_int_issue_peak(int device, float target_ms, double *warp_inst_per_s,
-                      double *ms, char *err, size_t errlen);
+/* Measures the device's integer issue peaks in warp instructions per second,
+ * the denominators of the search kernel's roofline: *issue_per_s with LOP3
+ * and IMAD interleaved (ALU and FMA pipes, the full issue rate) and
+ * *alu_per_s with LOP3 alone (the ALU pipe), each from independent chains at
+ * full occupancy over about target_ms. */
+int td_int_issue_peak(int device, float target_ms, double *issue_per_s,
+                      double *alu_per_s, char *err, size_t errlen);
 
 /* ---- serving: continuous batching ---------------------------------------- */
 

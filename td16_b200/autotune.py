@@ -27,10 +27,10 @@ TUNED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned.json")
 DEFAULT = {"warps": 4, "grain": 4, "split_level": 4, "check_every": 8}
 
 GRID = {
-    "warps": [2, 4, 8],
-    "grain": [1, 4, 16],
-    "split_level": [2, 4, 6],
-    "check_every": [8, 32, 128],
+    "warps": [4, 8],
+    "grain": [1, 2, 4],
+    "split_level": [2, 3, 4],
+    "check_every": [64, 256, 1024],
 }
 QUICK = {"warps": [2, 4], "grain": [4, 8], "split_level": [4], "check_every": [32, 128]}
 
@@ -67,10 +67,12 @@ def tune_bucket(slot: int, instances: np.ndarray, grid=None, repeats: int = 2, l
 
 
 def buckets(quick: bool):
-    """Sample workloads per bucket: the batched mix (n 11..13) and S_16."""
+    """Sample workloads per bucket: the batched mix (n 11..13) and S_16 (2^18
+    instances, so that the launch tail weighs about as much as in a full-size
+    batch)."""
     c = 4096 if quick else 16384
     mix = _lib.synth_perms(1, c, 11, 13, 25, 1, 3)
-    s16 = _lib.synth_perms(2, c, 16, 16, 50, 1, 4)
+    s16 = _lib.synth_perms(2, c if quick else 1 << 18, 16, 16, 50, 1, 4)
     return {
         "mix_11_13": _lib.prepare_perms(mix[0], mix[1], (mix[1] // 2 + 1).astype(np.int32)),
         "17": _lib.prepare_perms(s16[0], s16[1], 9),
@@ -93,7 +95,7 @@ def apply(bucket: str) -> dict:
 
 def main(argv):
     quick = "--quick" in argv
-    _lib.init_slots(1, [0], 256 << 20)
+    _lib.init_slots(1, [0], 2 << 30)
     out = {"when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()), "grid": QUICK if quick else GRID,
            "buckets": {}}
     try:

@@ -32,6 +32,7 @@
 #define TD_MAX_DEPTH 9   // moves (core/common.cuh:10-12)
 #define TD_MAX_TRIPLES 680
 #define TD_MAX_STEPS 22  // ceil(680 / 32)
+#define TD_MAX_ROUNDS 4  // ceil(C(16,2) / 32): pair slots of the bit-sliced evaluation
 #define TD_PT_STRIDE 32  // pair table row stride (bytes)
 
 // ---- C-ABI records (mirrored in include/td16_b200.h) ----------------------
@@ -158,6 +159,83 @@ TD_HD int td_class_of_index(int idx) {
     if (delta == 2) return TD_CLASS_PLUS2;
     if (delta == 0) return TD_CLASS_ZERO;
     return TD_CLASS_SKIP;
+}
+
+// ---- bit-sliced classification (free move order) ---------------------------
+//
+// The same classes for every third position k of a pair (i, j) at once, one
+// bit per k, from row masks of the node indexed by caller position:
+//   S[p] bit q: p and q lie on one omega cycle
+//   G[p] bit q: on one cycle and dist(p) > dist(q)
+//   P[p] bit q: on one cycle and the walk p -> q along omega has odd length
+//   O bit q:    q's cycle has odd length
+//   F bit q:    q is a fixed point
+// The entries of the pair table above follow from these: (i,j) = bits j of
+// rows i; (j,k) = rows j; and for (k,i), where the rows of i are read at k,
+// the walk k -> i is the rest of the cycle after the walk i -> k (its parity
+// is P[i] bit k xor O bit i) and dist(k) > dist(i) is the complement of G[i]
+// bit k.  With these entries the cases of td_class_of_index become:
+//   all three on one cycle: +2 when exactly two of dist(i)>dist(j),
+//     dist(j)>dist(k), dist(k)>dist(i) hold and at least two of the three walk
+//     parities are odd (their sum has the cycle's parity, so the change
+//     P1+P2+P3-O is then 2, else 0); otherwise 0;
+//   one pair on a cycle, the third symbol apart (walk parity s, cycle
+//     parities o1 of the pair and o2 of the lone symbol): filtered when the
+//     lone symbol is a fixed point; +2 when s & !o1 & !o2; filtered when
+//     !s & o1 & o2; 0 otherwise;
+//   three cycles: filtered.
+// Bits of k outside (j, N) are meaningless; the caller masks them.
+// The same with the per-lane flags already spread to full masks: oi/oj/fi/fj
+// are all-ones when i's/j's cycle is odd / i/j is fixed, and sh = 31 - j.
+TD_HD void td_row_classes_x(uint32_t Si, uint32_t Gi, uint32_t Pi, uint32_t Sj, uint32_t Gj, uint32_t Pj,
+                            uint32_t O, uint32_t F, uint32_t oi, uint32_t oj, uint32_t fi, uint32_t fj, int sh,
+                            uint32_t *plus2, uint32_t *zero) {
+    const uint32_t s1 = (uint32_t)((int32_t)(Si << sh) >> 31);   // i and j on one cycle
+    const uint32_t p1 = (uint32_t)((int32_t)(Pi << sh) >> 31);   // walk i -> j odd
+    const uint32_t g1 = (uint32_t)((int32_t)(Gi << sh) >> 31);   // dist(i) > dist(j)
+    const uint32_t P3 = Pi ^ oi;                 // walk k -> i odd (k on i's cycle)
+    // all three on one cycle (k on the common cycle of i and j)
+    const uint32_t G3 = ~Gi;                     // dist(k) > dist(i)
+    const uint32_t two = (g1 & Gj & ~G3) | (g1 & ~Gj & G3) | (~g1 & Gj & G3);
+    const uint32_t maj = (p1 & Pj) | (p1 & P3) | (Pj & P3);
+    const uint32_t all = s1 & Si;
+    const uint32_t split = two & maj;
+    // exactly one pair on a cycle: with s1 the pair is (i,j) and k lies apart;
+    // otherwise the pair is (j,k) where k is on j's cycle, (k,i) where on i's
+    const uint32_t sp = (s1 & p1) | (~s1 & ((Sj & Pj) | (~Sj & P3)));
+    const uint32_t o1 = (s1 & oi) | (~s1 & ((Sj & oj) | (~Sj & oi)));
+    const uint32_t o2 = (s1 & O) | (~s1 & ((Sj & oi) | (~Sj & oj)));
+    const uint32_t lf = (s1 & F) | (~s1 & ((Sj & fi) | (~Sj & fj)));
+    const uint32_t dom = (s1 & ~Si) | (~s1 & (Si | Sj));
+    const uint32_t p_one = dom & sp & ~o1 & ~o2 & ~lf;
+    const uint32_t z_one = dom & ~p_one & ~(lf | (~sp & o1 & o2));
+    *plus2 = (all & split) | p_one;
+    *zero = (all & ~split) | z_one;
+}
+
+TD_HD void td_row_classes(uint32_t Si, uint32_t Gi, uint32_t Pi, uint32_t Sj, uint32_t Gj, uint32_t Pj,
+                          uint32_t O, uint32_t F, int i, int j, uint32_t *plus2, uint32_t *zero) {
+    td_row_classes_x(Si, Gi, Pi, Sj, Gj, Pj, O, F, 0u - ((O >> i) & 1u), 0u - ((O >> j) & 1u),
+                     0u - ((F >> i) & 1u), 0u - ((F >> j) & 1u), 31 - j, plus2, zero);
+}
+
+// Pair slot q of a node with N positions: the pairs (i, j), i < j <= N-2 (the
+// first two positions of a triple), numbered so that higher slots hold
+// lexicographically smaller pairs.  Returns i | j << 5 | j << 10 | (31-j) << 15
+// (the third field is the shift of the k mask, k > j; the fourth brings bit j
+// to the sign bit), or 0 | 1 << 5 | 31 << 10 | 30 << 15 for a slot past the
+// last pair (an empty k mask).
+TD_HD uint32_t td_pair_code(int N, int q) {
+    const int NP = N < 3 ? 0 : (N - 1) * (N - 2) / 2;
+    if (q < 0 || q >= NP) return (1u << 5) | (31u << 10) | (30u << 15);
+    int rank = NP - 1 - q;  // lexicographic rank of the pair
+    int i = 0;
+    while (rank >= N - 2 - i) {  // pairs with first element i: j = i+1 .. N-2
+        rank -= N - 2 - i;
+        ++i;
+    }
+    const int j = i + 1 + rank;
+    return (uint32_t)i | ((uint32_t)j << 5) | ((uint32_t)j << 10) | ((uint32_t)(31 - j) << 15);
 }
 
 // Per-position cycle descriptor: leader (smallest pinned position of the

@@ -164,7 +164,7 @@ __device__ __forceinline__ int td_finish_unit(const td_dfs_out &r, td_inst_state
     return last;
 }
 
-__global__ void __launch_bounds__(256) td_steal_kernel(const td_instance *__restrict__ in,
+__global__ void __launch_bounds__(256, 4) td_steal_kernel(const td_instance *__restrict__ in,
                                                       td_result *__restrict__ out, int count, td_pool *pool,
                                                       td_item *items, uint32_t *ready, const uint32_t *epoch_ptr,
                                                       int capacity, td_inst_state *state, int grain,
@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(256) td_steal_kernel(const td_instance *__rest
                 td_write_result(&out[unit], td_instance_ok(x) ? TD_NOT_FOUND : TD_ERR_ARG, 0, 0, s.path, 0, 0, 8);
             } else {
                 if (lane == 0) atomicAdd(&st->pending, 1);
-                td_setup_root(s, x, code, codeN);
+                td_setup_root<false>(s, x, code, codeN);
                 dc.inst = (uint32_t)unit;
                 dc.state = st;
                 const td_dfs_out r = td_dfs<false>(s, lut, code, x.n_symbols, x.max_moves, 0, lim, &dc);
@@ -277,7 +277,7 @@ __global__ void __launch_bounds__(256) td_steal_kernel(const td_instance *__rest
                 const uint32_t idx = it.inst;
                 const td_instance x = in[idx];
                 td_inst_state *st = &state[idx];
-                td_setup_root(s, x, code, codeN);
+                td_setup_root<false>(s, x, code, codeN);
                 const int d0 = it.depth;
                 if (lane == 0) {
                     s.L[d0] = it.L;
@@ -345,18 +345,27 @@ __global__ void td_validate_kernel(const td_instance *__restrict__ in, td_result
     if (mark && r.status == TD_FOUND && !good) res[idx].status = TD_ERR_VERIFY;
 }
 
-// Integer issue peak: independent LOP3 chains (ALU pipe) at full occupancy.
-// Each thread runs `iters` iterations of 16 lop3 operations over 8 registers.
+// Integer issue peaks at full occupancy.  Each thread runs `iters` iterations
+// of 16 operations over 8 independent chains.  MIX = 0: LOP3 only (ALU pipe
+// alone, 16 lanes per SM sub-partition, so at most half a warp instruction per
+// clock per sub-partition).  MIX = 1: LOP3 and IMAD alternate (ALU and FMA
+// pipes side by side), which can reach one warp instruction per clock per
+// sub-partition: the full issue rate.
+template <int MIX>
 __global__ void __launch_bounds__(256) td_int_peak_kernel(uint32_t *sink, int iters) {
     uint32_t a[8];
 #pragma unroll
     for (int c = 0; c < 8; ++c) a[c] = threadIdx.x * 0x9E3779B9u + c * 0x85EBCA6Bu + blockIdx.x;
+    const uint32_t m = 0x01000193u | (blockIdx.x << 1);
     for (int it = 0; it < iters; ++it) {
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
 #pragma unroll
             for (int c = 0; c < 8; ++c) {
-                asm volatile("lop3.b32 %0, %0, %1, %2, 0x96;" : "+r"(a[c]) : "r"(a[(c + 1) & 7]), "r"(a[(c + 3) & 7]));
+                if (MIX && (c & 1))
+                    asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a[c]) : "r"(m), "r"(a[(c + 3) & 7]));
+                else
+                    asm volatile("lop3.b32 %0, %0, %1, %2, 0x96;" : "+r"(a[c]) : "r"(a[(c + 1) & 7]), "r"(a[(c + 3) & 7]));
             }
         }
     }
@@ -412,6 +421,10 @@ int g_grain = 1;            // instances per ticket (ordered persistent kernel)
 int g_steal_grain = 4;      // items per donation
 int g_split_level = 4;      // donate children of levels <= this
 int g_check_every = 8;      // expansions between idle checks
+// the same for serving launches, where latency rather than throughput counts
+int g_serve_grain = 1;
+int g_serve_split_level = 2;
+int g_serve_check_every = 32;
 
 void set_err(char *err, size_t len, const std::string &msg) {
     if (err && len) {
@@ -838,6 +851,18 @@ TD_API int td_configure_steal(int grain, int split_level, int check_every) {
     return TD_OK;
 }
 
+// Work distribution of later serving launches (td_serve_open): items per
+// donation, deepest level whose children are donated, expansions between
+// idle checks.
+TD_API int td_configure_serve(int grain, int split_level, int check_every) {
+    if (grain < 1 || split_level < 0 || split_level >= TD_MAX_DEPTH || check_every < 1) return TD_INVALID_ARG;
+    std::lock_guard<std::mutex> g(g_mu);
+    g_serve_grain = grain;
+    g_serve_split_level = split_level;
+    g_serve_check_every = check_every;
+    return TD_OK;
+}
+
 TD_API int td_prepare_pairs(int count, const uint8_t *beta, const uint8_t *omega, const uint8_t *n,
                             const int32_t *init, const float *min_rate, const int32_t *max_moves,
                             const uint8_t *full, td_instance *out, int *bad) {
@@ -1016,39 +1041,60 @@ TD_API void td_positions_to_symbols(const uint8_t *beta, int n, const int16_t *i
     }
 }
 
-// Measures the ALU-pipe integer issue rate of `device` in warp instructions
-// per second (LOP3 only), at full occupancy, over about `target_ms`.
-TD_API int td_int_issue_peak(int device, float target_ms, double *warp_inst_per_s, double *ms_out, char *err,
+namespace {
+
+// Times one form of td_int_peak_kernel on the current device, doubling the
+// iteration count until a launch lasts `target_ms`; returns warp instructions
+// per second.
+template <int MIX>
+int time_int_peak(int sms, float target_ms, uint32_t *sink, cudaEvent_t a, cudaEvent_t b, double *rate) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, td_int_peak_kernel<MIX>, 256, 0) != cudaSuccess)
+        return -1;
+    const int blocks = sms * std::max(1, per_sm);
+    int iters = 1024;
+    float ms = 0;
+    for (int attempt = 0; attempt < 12; ++attempt) {
+        td_int_peak_kernel<MIX><<<blocks, 256>>>(sink, iters);  // warm-up at this size
+        cudaEventRecord(a);
+        td_int_peak_kernel<MIX><<<blocks, 256>>>(sink, iters);
+        cudaEventRecord(b);
+        if (cudaEventSynchronize(b) != cudaSuccess || cudaEventElapsedTime(&ms, a, b) != cudaSuccess) return -1;
+        if (ms >= target_ms) break;
+        iters *= 2;
+    }
+    *rate = (double)blocks * (256 / 32) * (double)iters * 16.0 / (ms * 1e-3);
+    return 0;
+}
+
+}  // namespace
+
+// Measures the integer issue peaks of `device` in warp instructions per
+// second: the full issue rate (LOP3 and IMAD interleaved) and the ALU-pipe
+// rate (LOP3 only), each over about `target_ms`.
+TD_API int td_int_issue_peak(int device, float target_ms, double *issue_per_s, double *alu_per_s, char *err,
                              size_t errlen) {
     TD_CHECK(cudaSetDevice(device));
     int sms = 0;
     TD_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    int per_sm = 0;
-    TD_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, td_int_peak_kernel, 256, 0));
-    const int blocks = sms * std::max(1, per_sm);
     uint32_t *sink = nullptr;
-    TD_CHECK(cudaMalloc(&sink, sizeof(uint32_t) * blocks));
+    TD_CHECK(cudaMalloc(&sink, sizeof(uint32_t) * sms * 32));
     cudaEvent_t a, b;
     TD_CHECK(cudaEventCreate(&a));
     TD_CHECK(cudaEventCreate(&b));
-    int iters = 1024;
-    float ms = 0;
-    for (int attempt = 0; attempt < 12; ++attempt) {
-        td_int_peak_kernel<<<blocks, 256>>>(sink, iters);  // warm-up at this size
-        TD_CHECK(cudaEventRecord(a));
-        td_int_peak_kernel<<<blocks, 256>>>(sink, iters);
-        TD_CHECK(cudaEventRecord(b));
-        TD_CHECK(cudaEventSynchronize(b));
-        TD_CHECK(cudaEventElapsedTime(&ms, a, b));
-        if (ms >= target_ms) break;
-        iters *= 2;
-    }
+    double issue = 0, alu = 0;
+    const int rc = (time_int_peak<1>(sms, target_ms, sink, a, b, &issue) == 0 &&
+                    time_int_peak<0>(sms, target_ms, sink, a, b, &alu) == 0) ? 0 : -1;
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     cudaFree(sink);
-    const double warp_insts = (double)blocks * (256 / 32) * (double)iters * 16.0;
-    if (warp_inst_per_s) *warp_inst_per_s = warp_insts / (ms * 1e-3);
-    if (ms_out) *ms_out = ms;
+    TD_CHECK(cudaGetLastError());
+    if (rc != 0) {
+        set_err(err, errlen, "td_int_issue_peak: a probe launch failed");
+        return TD_CUDA_ERROR;
+    }
+    if (issue_per_s) *issue_per_s = issue;
+    if (alu_per_s) *alu_per_s = alu;
     return TD_OK;
 }
 

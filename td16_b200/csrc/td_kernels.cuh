@@ -28,12 +28,28 @@ __device__ __forceinline__ int td_group_of(int b) { return (b * 11) >> 5; }
 
 // Per-warp shared state.
 struct td_warp_smem {
-    uint8_t pt[TD_PT_ROWS * TD_PT_STRIDE];     // pair table of the current node
-    // per level, per lane: the outcome of every step in 3-bit groups, ten
-    // steps per word (step st in word st/10 at bit 3*(st%10)): bit 0 found
-    // (accepted root in ordered mode), bit 1 first-choice child, bit 2
-    // second-choice child
-    uint32_t pm[TD_MAX_DEPTH][3][32];
+    union {
+        struct {  // reference move order (one triple per lane and step)
+            uint8_t pt[TD_PT_ROWS * TD_PT_STRIDE];     // pair table of the current node
+            // per level, per lane: the outcome of every step in 3-bit groups, ten
+            // steps per word (step st in word st/10 at bit 3*(st%10)): bit 0 found
+            // (accepted root in ordered mode), bit 1 first-choice child, bit 2
+            // second-choice child
+            uint32_t pm[TD_MAX_DEPTH][3][32];
+        };
+        struct {  // free move order (bit-sliced: one pair and all its k per lane and round)
+            uint4 rows[TD_MAX_N];                      // per caller position: S, G, P row masks
+            // per level and lane: the expandable children of the lane's four
+            // pair slots (word r = slot 4*lane + r), +2 class at bits k-1
+            // (1..15), 0 class at bits k+15 (17..31)
+            uint4 pw[TD_MAX_DEPTH][32];
+            uint32_t m2[TD_MAX_DEPTH];                 // per level: lanes that hold +2 children
+            uint32_t m0[TD_MAX_DEPTH];                 // per level: lanes that hold 0 children
+            // per level: the caller's array, one pinned label per caller position
+            uint8_t A[TD_MAX_DEPTH + 1][32];
+            uint8_t inv[32];                           // caller position of each label
+        };
+    };
     uint64_t L[TD_MAX_DEPTH + 1];              // pinned state per level
     uint32_t acc[TD_MAX_DEPTH + 2];            // accept mask over odd counts, per depth
     uint32_t reach[TD_MAX_DEPTH + 2];          // prune mask over odd counts, per depth
@@ -280,6 +296,225 @@ __device__ __forceinline__ int td_next_child(td_warp_smem &s, int level, int *ac
     return st * 32 + win;
 }
 
+// ---- free move order: bit-sliced evaluation ---------------------------------
+//
+// The state of a level is the caller's array, one byte per caller position
+// holding the pinned label (A[c] = B[(c + off) mod N]).  In these terms omega
+// maps A[c] to A[c-1] + 1 (mod N), and a move (i, j, k) is the plain block swap
+// A[:i] + A[j:k] + A[i:j] + A[k:] (the pinned form's start-of-array rule is the
+// rotation that keeps label 0 first).  Lane l owns pair slots 4 l + r
+// (td_pair_code) and classifies the children (i, j, k) of every k at once
+// from the node's row masks (td_row_classes).
+
+// Rounds of the bit-sliced evaluation for N: ceil(C(N-1,2) / 32).
+__device__ __forceinline__ int td_pair_rounds(int N) {
+    const int NP = N < 3 ? 0 : (N - 1) * (N - 2) / 2;
+    return (NP + 31) >> 5;
+}
+
+// Lane l owns slots R l + r, r < R = td_pair_rounds(N); code[r] for r >= R
+// (and code[TD_MAX_ROUNDS]) holds R.
+__device__ __forceinline__ void td_load_pairs(int N, uint32_t (&code)[TD_MAX_STEPS]) {
+    const int lane = threadIdx.x & 31;
+    const int R = td_pair_rounds(N);
+#pragma unroll
+    for (int r = 0; r < TD_MAX_ROUNDS; ++r) code[r] = td_pair_code(N, r < R ? R * lane + r : -1);
+    code[TD_MAX_ROUNDS] = (uint32_t)R;
+}
+
+// Pinned state (L, off) -> the caller's array of `level`.
+__device__ __forceinline__ void td_unpack_state(td_warp_smem &s, int level, uint64_t L, int off, int N) {
+    const int c = threadIdx.x & 31;
+    if (c < N) {
+        int p = c + off;
+        p -= p >= N ? N : 0;
+        s.A[level][c] = (uint8_t)(p ? td_nib(L, p - 1) + 1u : 0u);
+    }
+    __syncwarp();
+}
+
+// The caller's array of `level` -> pinned state (L, off): label 0 sits at
+// caller position c0, so off = -c0 mod N and L[m] = A[(m + 1 + c0) mod N] - 1.
+__device__ __forceinline__ void td_pack_state(const td_warp_smem &s, int level, int N, uint64_t *L, int *off) {
+    const int m = threadIdx.x & 31;
+    const uint32_t z = __ballot_sync(TD_FULL, m < N && s.A[level][m] == 0);
+    const int c0 = __ffs(z) - 1;
+    uint32_t lo = 0, hi = 0;
+    if (m < 16) {
+        uint32_t v = (uint32_t)m;
+        if (m < N - 1) {
+            int q = m + 1 + c0;
+            q -= q >= N ? N : 0;
+            v = s.A[level][q] - 1u;
+        }
+        const uint64_t w = (uint64_t)v << (4 * m);
+        lo = (uint32_t)w;
+        hi = (uint32_t)(w >> 32);
+    }
+    lo = __reduce_or_sync(TD_FULL, lo);
+    hi = __reduce_or_sync(TD_FULL, hi);
+    *L = ((uint64_t)hi << 32) | lo;
+    *off = c0 == 0 ? 0 : N - c0;
+}
+
+// The caller's array of level+1 = that of `level` after the move t.
+__device__ __forceinline__ void td_apply_bytes(td_warp_smem &s, int level, uint32_t t, int N) {
+    const int m = threadIdx.x & 31;
+    const int i = t & 31, j = (t >> 5) & 31, k = (t >> 10) & 31;
+    if (m < N) {
+        int src = m;
+        if (m >= i && m < k) src = m < i + (k - j) ? m + (j - i) : m - (k - j);
+        s.A[level + 1][m] = s.A[level][src];
+    }
+    __syncwarp();
+}
+
+// Row masks of the node at `level` (lane c = caller position c); returns the
+// number of odd-length omega cycles and the odd-cycle and fixed-point masks.
+__device__ __forceinline__ int td_prepare_rows(td_warp_smem &s, int level, int N, uint32_t &O, uint32_t &F) {
+    const int c = threadIdx.x & 31;
+    const bool act = c < N;
+    const int a = act ? s.A[level][c] : 0;
+    const int am1 = __shfl_sync(TD_FULL, a, c == 0 ? N - 1 : c - 1);
+    if (act) s.inv[a] = (uint8_t)c;
+    __syncwarp();
+    // next caller position along omega: the one holding A[c-1] + 1 (mod N)
+    const int y = am1 + 1 == N ? 0 : am1 + 1;
+    const int nx = act ? (int)s.inv[y] : c;
+    // leader (smallest caller position on the cycle) and dist (omega steps to
+    // it) in one pointer-jumping pass: each lane keeps the minimum of the
+    // window c, next(c), ..., next^(w-1)(c) and its distance; windows double
+    // per round and 32 >= any cycle length, so the first occurrence wins.
+    int m = c, d = 0, j = nx;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+        const int mB = __shfl_sync(TD_FULL, m, j);
+        const int dB = __shfl_sync(TD_FULL, d, j);
+        const int jB = __shfl_sync(TD_FULL, j, j);
+        if (mB < m) {
+            m = mB;
+            d = (1 << r) + dB;
+        }
+        j = jB;
+    }
+    const int after_leader = __shfl_sync(TD_FULL, nx, m);
+    const int len = __shfl_sync(TD_FULL, d, after_leader) + 1;
+    const uint32_t ACT = (1u << N) - 1u;
+    const uint32_t S = __match_any_sync(TD_FULL, m) & ACT;  // inactive lanes are their own leaders
+    // lt bit q: dist(q) < dist(c), by comparing the five bit planes of dist
+    uint32_t lt = 0, eq = TD_FULL, D0 = 0;
+#pragma unroll
+    for (int b = 4; b >= 0; --b) {
+        const uint32_t Bb = __ballot_sync(TD_FULL, (d >> b) & 1);
+        const uint32_t mb = 0u - (uint32_t)((d >> b) & 1);
+        lt |= eq & ~Bb & mb;
+        eq &= ~(Bb ^ mb);
+        if (b == 0) D0 = Bb;
+    }
+    const uint32_t lodd = 0u - (uint32_t)(len & 1);
+    const uint32_t G = S & lt;
+    // walk c -> q: dist(c) - dist(q), plus the cycle length when q is further
+    const uint32_t P = S & ((D0 ^ (0u - (uint32_t)(d & 1))) ^ (lodd & ~lt));
+    O = __ballot_sync(TD_FULL, act && (len & 1));
+    F = __ballot_sync(TD_FULL, act && len == 1);
+    const int odd = __popc(__ballot_sync(TD_FULL, act && m == c && (len & 1)));
+    // fourth word: byte 0 = 0xff when c's cycle is odd, byte 1 = 0xff when c is fixed
+    const uint32_t flags = ((len & 1) ? 0x00ffu : 0u) | (len == 1 ? 0xff00u : 0u);
+    if (act) s.rows[c] = make_uint4(S, G, P, flags);
+    __syncwarp();
+    return odd;
+}
+
+// Classifies every child of the node at `level`; fills the level's outcome
+// words and lane summaries and returns a found move (i | j<<5 | k<<10) or -1.
+__device__ __forceinline__ int td_evaluate_rows(td_warp_smem &s, const uint32_t (&code)[TD_MAX_STEPS], int N,
+                                                int level, int odd, uint32_t O, uint32_t F) {
+    const int lane = threadIdx.x & 31;
+    const int D = level + 1;
+    const uint32_t accD = s.acc[D], reachD = s.reach[D];
+    const uint32_t f0 = 0u - ((accD >> odd) & 1u), f2 = 0u - ((accD >> (odd + 2)) & 1u);
+    const uint32_t x0 = (0u - ((reachD >> odd) & 1u)) & ~f0;
+    const uint32_t x2 = (0u - ((reachD >> (odd + 2)) & 1u)) & ~f2;
+    const uint32_t ACT = (1u << N) - 1u;
+    const bool accepting = (f0 | f2) != 0;  // warp-uniform
+    const int R = (int)code[TD_MAX_ROUNDS];  // warp-uniform
+    uint32_t key = 0xffffffffu;
+    uint32_t W[TD_MAX_ROUNDS] = {0u, 0u, 0u, 0u};
+#pragma unroll
+    for (int r = 0; r < TD_MAX_ROUNDS; ++r) {
+        if (r >= R) break;
+        const uint32_t pc = code[r];
+        const int i = pc & 31, j = (pc >> 5) & 31, ks = (pc >> 10) & 31;
+        const uint4 ri = s.rows[i], rj = s.rows[j];
+        uint32_t plus, zero;
+        td_row_classes_x(ri.x, ri.y, ri.z, rj.x, rj.y, rj.z, O, F, __byte_perm(ri.w, 0, 0x0000),
+                         __byte_perm(rj.w, 0, 0x0000), __byte_perm(ri.w, 0, 0x1111), __byte_perm(rj.w, 0, 0x1111),
+                         (int)(pc >> 15), &plus, &zero);
+        const uint32_t km = ACT & (0xfffffffeu << ks);
+        W[r] = ((km & x2 & plus) >> 1) | ((km & x0 & zero) << 15);
+        if (accepting) {
+            const uint32_t fnd = km & ((f0 & zero) | (f2 & plus));
+            if (fnd && key == 0xffffffffu)
+                key = ((uint32_t)lane << 17) | ((uint32_t)r << 15) | (pc & 1023u) |
+                      ((uint32_t)(31 - __clz(fnd)) << 10);
+        }
+    }
+    s.pw[level][lane] = make_uint4(W[0], W[1], W[2], W[3]);
+    const uint32_t any = W[0] | W[1] | W[2] | W[3];
+    const uint32_t m2 = __ballot_sync(TD_FULL, (any & 0x0000ffffu) != 0);
+    const uint32_t m0 = __ballot_sync(TD_FULL, (any & 0xffff0000u) != 0);
+    if (lane == 0) {
+        s.m2[level] = m2;
+        s.m0[level] = m0;
+    }
+    if (accepting) {
+        key = __reduce_min_sync(TD_FULL, key);
+        if (key != 0xffffffffu) {
+            __syncwarp();
+            return (int)(key & 0x7fffu);
+        }
+    }
+    __syncwarp();
+    return -1;
+}
+
+// Next child of `level` in the free order: +2 children first; among them the
+// highest pair slot (the lexicographically smallest pair) and its smallest k.
+// Returns the move or -1.
+__device__ __forceinline__ int td_next_child_rows(td_warp_smem &s, const uint32_t (&code)[TD_MAX_STEPS],
+                                                  int level) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t m2 = s.m2[level], m0 = s.m0[level];
+    if ((m2 | m0) == 0) return -1;
+    const bool c2 = m2 != 0;
+    const uint32_t lanes = c2 ? m2 : m0;
+    const int win = 31 - __clz(lanes);
+    const uint4 Wv = s.pw[level][win];
+    const uint32_t cm = c2 ? 0x0000ffffu : 0xffff0000u;
+    int r;
+    uint32_t w;
+    if (Wv.w & cm) { r = 3; w = Wv.w; }
+    else if (Wv.z & cm) { r = 2; w = Wv.z; }
+    else if (Wv.y & cm) { r = 1; w = Wv.y; }
+    else { r = 0; w = Wv.x; }
+    const int b = __ffs(w & cm) - 1;
+    const uint32_t nw = w & ~(1u << b);
+    const uint32_t mine = r == 3 ? code[3] : (r == 2 ? code[2] : (r == 1 ? code[1] : code[0]));
+    const uint32_t pc = __shfl_sync(TD_FULL, mine, win);
+    // does the winning lane keep children of this class?
+    const uint32_t rest = (r == 0 ? nw : Wv.x) | (r == 1 ? nw : Wv.y) | (r == 2 ? nw : Wv.z) | (r == 3 ? nw : Wv.w);
+    if (lane == 0) {
+        reinterpret_cast<uint32_t *>(&s.pw[level][win])[r] = nw;
+        if (!(rest & cm)) {
+            if (c2) s.m2[level] = m2 & ~(1u << win);
+            else s.m0[level] = m0 & ~(1u << win);
+        }
+    }
+    __syncwarp();
+    const int k = c2 ? b + 1 : b - 15;
+    return (int)((pc & 1023u) | ((uint32_t)k << 10));
+}
+
 // ---- work items (subtree roots handed between warps) ----------------------
 
 // A node that is known to be expandable, with the moves that lead to it.
@@ -346,20 +581,20 @@ struct td_dfs_out {
 };
 
 // Hands some remaining children of the shallowest level in [d0, level] to the
-// pool as items.  Returns the number donated (uniform across the warp).
-__device__ __forceinline__ int td_donate(td_warp_smem &s, const td_donate_ctx &dc, int d0, int level, int N,
-                                         int T, int tri_base, int want) {
+// pool as items (free move order).  Returns the number donated (uniform
+// across the warp).
+__device__ __forceinline__ int td_donate(td_warp_smem &s, const td_donate_ctx &dc,
+                                         const uint32_t (&code)[TD_MAX_STEPS], int d0, int level, int N,
+                                         int want) {
     const int lane = threadIdx.x & 31;
-    const uint32_t CAND = TD_G1 | TD_G2;
     int lv = -1;
     for (int l = d0; l <= level && l <= dc.max_level; ++l) {
-        const uint32_t w = (s.pm[l][0][lane] | s.pm[l][1][lane] | s.pm[l][2][lane]) & CAND;
-        if (__any_sync(TD_FULL, w != 0)) { lv = l; break; }
+        if (s.m2[l] | s.m0[l]) { lv = l; break; }
     }
     if (lv < 0) return 0;
-    uint32_t P0 = s.pm[lv][0][lane], P1 = s.pm[lv][1][lane], P2 = s.pm[lv][2][lane];
-    uint32_t Q0 = P0 & CAND, Q1 = P1 & CAND, Q2 = P2 & CAND;
-    const int cnt = __popc(Q0) + __popc(Q1) + __popc(Q2);
+    const uint4 Wv = s.pw[lv][lane];
+    uint32_t W0 = Wv.x, W1 = Wv.y, W2 = Wv.z, W3 = Wv.w;
+    const int cnt = __popc(W0) + __popc(W1) + __popc(W2) + __popc(W3);
     const int have = __reduce_add_sync(TD_FULL, (unsigned)cnt);
     // leave at least one child to this warp when the level is the current one
     const int give = min(want, have - (lv == level ? 1 : 0));
@@ -395,22 +630,23 @@ __device__ __forceinline__ int td_donate(td_warp_smem &s, const td_donate_ctx &d
         atomicAdd(&dc.pool->donations, 1ull);
         atomicAdd(&dc.pool->donated_items, (unsigned long long)give);
     }
+    uint64_t Lp;
+    int offp;
+    td_pack_state(s, lv, N, &Lp, &offp);  // the parent in pinned form
     int slot = base + before;
+    // a lane gives its lowest slots first (the ones this warp visits last),
+    // and 0-class children (high bits) before +2 children
     for (int taken = 0; taken < mine; ++taken) {
-        int k, b;
-        if (Q0) { k = 0; b = __ffs(Q0) - 1; Q0 &= Q0 - 1; }
-        else if (Q1) { k = 1; b = __ffs(Q1) - 1; Q1 &= Q1 - 1; }
-        else { k = 2; b = __ffs(Q2) - 1; Q2 &= Q2 - 1; }
-        const int j = td_group_of(b);
-        const uint32_t clear = ~(7u << (3 * j));
-        if (k == 0) P0 &= clear;
-        else if (k == 1) P1 &= clear;
-        else P2 &= clear;
-        const int u = 32 * (10 * k + j) + lane;
-        const uint32_t t = td_tri_table[tri_base + T - 1 - u];
+        uint32_t pc, b;
+        if (W0) { pc = code[0]; b = 31 - __clz(W0); W0 &= ~(1u << b); }
+        else if (W1) { pc = code[1]; b = 31 - __clz(W1); W1 &= ~(1u << b); }
+        else if (W2) { pc = code[2]; b = 31 - __clz(W2); W2 &= ~(1u << b); }
+        else { pc = code[3]; b = 31 - __clz(W3); W3 &= ~(1u << b); }
+        const uint32_t k = b < 16 ? b + 1 : b - 15;
+        const uint32_t t = (pc & 1023u) | (k << 10);
         uint64_t nL;
         int noff;
-        td_apply_move(s.L[lv], s.off[lv], N, t & 31, (t >> 5) & 31, (t >> 10) & 31, &nL, &noff);
+        td_apply_move(Lp, offp, N, t & 31, (t >> 5) & 31, (t >> 10) & 31, &nL, &noff);
         td_item it;
         it.L = nL;
         it.inst = dc.inst;
@@ -438,15 +674,23 @@ __device__ __forceinline__ int td_donate(td_warp_smem &s, const td_donate_ctx &d
         atomicExch(&dc.ready[phys], tag);
         ++slot;
     }
-    s.pm[lv][0][lane] = P0;
-    s.pm[lv][1][lane] = P1;
-    s.pm[lv][2][lane] = P2;
+    s.pw[lv][lane] = make_uint4(W0, W1, W2, W3);
+    const uint32_t any = W0 | W1 | W2 | W3;
+    const uint32_t m2 = __ballot_sync(TD_FULL, (any & 0x0000ffffu) != 0);
+    const uint32_t m0 = __ballot_sync(TD_FULL, (any & 0xffff0000u) != 0);
+    if (lane == 0) {
+        s.m2[lv] = m2;
+        s.m0[lv] = m0;
+    }
     __syncwarp();
     return give;
 }
 
 // Depth-first search from the node held at level d0 of `s` (state, path and
-// rate masks already set).  Leaves the frames intact on TD_DFS_BUDGET.
+// rate masks already set).  Leaves the frames intact on TD_DFS_BUDGET.  The
+// reference order evaluates one triple per lane and step (`code` holds the
+// lane's triple codes); the free order is bit-sliced (`code` holds the lane's
+// pair slots) and may donate subtrees through `dc`.
 template <bool ORDERED>
 __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t (&code)[TD_MAX_STEPS],
                              int N, int maxd, int d0, const td_search_limits &lim, const td_donate_ctx *dc) {
@@ -460,12 +704,22 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
     r.found_move = 0;
     r.expansions = 0;
     int level = d0;
-    int odd = td_prepare_node(s, s.L[d0], s.off[d0], N);
-    int found = td_evaluate<ORDERED>(s, lut, code, steps, d0, odd, maxd);
+    uint32_t O = 0, F = 0;
+    int found;
+    if constexpr (ORDERED) {
+        const int odd = td_prepare_node(s, s.L[d0], s.off[d0], N);
+        found = td_evaluate<true>(s, lut, code, steps, d0, odd, maxd);
+        if (found >= 0) found = td_tri_table[tri_base + T - 1 - found];
+    } else {
+        td_unpack_state(s, d0, s.L[d0], s.off[d0], N);
+        const int odd = td_prepare_rows(s, d0, N, O, F);
+        found = td_evaluate_rows(s, code, N, d0, odd, O, F);
+    }
     r.expansions = 1;
+    int since_check = 0;
     for (;;) {
         if (found >= 0) {
-            r.found_move = (uint16_t)td_tri_table[tri_base + T - 1 - found];
+            r.found_move = (uint16_t)found;
             r.depth = level + 1;
             r.status = TD_DFS_FOUND;
             break;
@@ -474,19 +728,26 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
             r.status = TD_DFS_BUDGET;
             break;
         }
-        if (dc && (r.expansions % (uint32_t)dc->check_every) == 0) {
-            int hungry = 0, stop = 0;
-            if (lane == 0) {
-                hungry = *(volatile int *)&dc->pool->idle;
-                stop = *(volatile int *)&dc->state->found;
+        if constexpr (!ORDERED) {
+            if (dc && ++since_check >= dc->check_every) {
+                since_check = 0;
+                int hungry = 0, stop = 0;
+                if (lane == 0) {
+                    // idle warps not yet served by an unclaimed item: without
+                    // this, every busy warp would donate to the same few idle ones
+                    const int idle = *(volatile int *)&dc->pool->idle;
+                    const int unclaimed = *(volatile int *)&dc->pool->produced - *(volatile int *)&dc->pool->consumed;
+                    hungry = idle - unclaimed;
+                    stop = *(volatile int *)&dc->state->found;
+                }
+                stop = __shfl_sync(TD_FULL, stop, 0);
+                if (stop) {
+                    r.status = TD_DFS_ABORTED;
+                    break;
+                }
+                hungry = __shfl_sync(TD_FULL, hungry, 0);
+                if (hungry > 0) td_donate(s, *dc, code, d0, level, N, min(hungry, dc->grain));
             }
-            stop = __shfl_sync(TD_FULL, stop, 0);
-            if (stop) {
-                r.status = TD_DFS_ABORTED;
-                break;
-            }
-            hungry = __shfl_sync(TD_FULL, hungry, 0);
-            if (hungry > 0) td_donate(s, *dc, d0, level, N, T, tri_base, min(hungry, dc->grain));
         }
         if ((r.expansions & 255u) == 0) {
             int stop = 0;
@@ -499,32 +760,52 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
                 break;
             }
         }
-        int accepted;
-        const int u = td_next_child<ORDERED>(s, level, &accepted);
-        if (u < 0) {
-            if (level == d0) break;  // this subtree is exhausted
-            --level;
-            continue;
+        uint32_t t;
+        if constexpr (ORDERED) {
+            int accepted;
+            const int u = td_next_child<true>(s, level, &accepted);
+            if (u < 0) {
+                if (level == d0) break;  // this subtree is exhausted
+                --level;
+                continue;
+            }
+            t = td_tri_table[tri_base + T - 1 - u];
+            if (accepted) {
+                r.found_move = (uint16_t)t;
+                r.depth = level + 1;
+                r.status = TD_DFS_FOUND;
+                break;
+            }
+        } else {
+            const int m = td_next_child_rows(s, code, level);
+            if (m < 0) {
+                if (level == d0) break;  // this subtree is exhausted
+                --level;
+                continue;
+            }
+            t = (uint32_t)m;
         }
-        const uint32_t t = td_tri_table[tri_base + T - 1 - u];
-        if (accepted) {
-            r.found_move = (uint16_t)t;
-            r.depth = level + 1;
-            r.status = TD_DFS_FOUND;
-            break;
+        if constexpr (ORDERED) {
+            uint64_t nL;
+            int noff;
+            td_apply_move(s.L[level], s.off[level], N, t & 31, (t >> 5) & 31, (t >> 10) & 31, &nL, &noff);
+            __syncwarp();
+            if (lane == 0) {
+                s.path[level] = (uint16_t)t;
+                s.L[level + 1] = nL;
+                s.off[level + 1] = (uint8_t)noff;
+            }
+            ++level;
+            const int odd = td_prepare_node(s, nL, noff, N);
+            found = td_evaluate<true>(s, lut, code, steps, level, odd, maxd);
+            if (found >= 0) found = td_tri_table[tri_base + T - 1 - found];
+        } else {
+            if (lane == 0) s.path[level] = (uint16_t)t;
+            td_apply_bytes(s, level, t, N);
+            ++level;
+            const int odd = td_prepare_rows(s, level, N, O, F);
+            found = td_evaluate_rows(s, code, N, level, odd, O, F);
         }
-        uint64_t nL;
-        int noff;
-        td_apply_move(s.L[level], s.off[level], N, t & 31, (t >> 5) & 31, (t >> 10) & 31, &nL, &noff);
-        __syncwarp();
-        if (lane == 0) {
-            s.path[level] = (uint16_t)t;
-            s.L[level + 1] = nL;
-            s.off[level + 1] = (uint8_t)noff;
-        }
-        ++level;
-        odd = td_prepare_node(s, nL, noff, N);
-        found = td_evaluate<ORDERED>(s, lut, code, steps, level, odd, maxd);
         ++r.expansions;
     }
     __syncwarp();
@@ -536,13 +817,19 @@ __device__ __forceinline__ bool td_instance_ok(const td_instance &x) {
            td_inst_init(x) <= TD_MAX_N;
 }
 
-// Loads codes for N and the instance's rate masks; places its root at level 0.
+// Loads the lane's codes for N (triple codes in the reference order, pair
+// slots in the free order) and the instance's rate masks; places its root at
+// level 0.  `codeN` caches the N the codes were loaded for (negative for the
+// other order's codes).
+template <bool ORDERED>
 __device__ __forceinline__ void td_setup_root(td_warp_smem &s, const td_instance &x, uint32_t (&code)[TD_MAX_STEPS],
                                               int &codeN) {
     const int lane = threadIdx.x & 31;
-    if (codeN != x.n_symbols) {
-        td_load_codes(x.n_symbols, code);
-        codeN = x.n_symbols;
+    const int want = ORDERED ? x.n_symbols : -1 - x.n_symbols;
+    if (codeN != want) {
+        if constexpr (ORDERED) td_load_codes(x.n_symbols, code);
+        else td_load_pairs(x.n_symbols, code);
+        codeN = want;
     }
     td_rate_masks(s, x);
     if (lane == 0) {
@@ -584,7 +871,7 @@ __device__ void td_warp_search(const td_instance &x, td_result *out, td_warp_sme
     if (!td_instance_ok(x)) {
         status = TD_ERR_ARG;
     } else if (td_triple_count(x.n_symbols) > 0) {
-        td_setup_root(s, x, code, codeN);
+        td_setup_root<ORDERED>(s, x, code, codeN);
         const td_dfs_out r = td_dfs<ORDERED>(s, lut, code, x.n_symbols, x.max_moves, 0, lim, nullptr);
         expansions = r.expansions;
         if (r.status == TD_DFS_FOUND) {

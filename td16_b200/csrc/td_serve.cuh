@@ -32,7 +32,7 @@ struct td_serve_dev_ctl {      // device memory: scheduler state of the launch
 // single warp for its whole search.  The warp that finishes a request last
 // writes its result and stamps done[slot] = request + 1.
 template <bool ORDERED>
-__global__ void __launch_bounds__(256) td_serve_kernel(const td_instance *ring, td_result *results,
+__global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *ring, td_result *results,
                                                       volatile unsigned long long *done, unsigned ring_size,
                                                       td_serve_host_ctl *hctl, td_serve_dev_ctl *dctl,
                                                       td_instance *queue, td_inst_state *state, td_pool *pool,
@@ -104,20 +104,25 @@ __global__ void __launch_bounds__(256) td_serve_kernel(const td_instance *ring, 
         int kind = 0;
         long long unit = -1;
         if (lane == 0) {
-            const unsigned long long av = *(volatile unsigned long long *)&dctl->available;
-            unsigned long long c = *(volatile unsigned long long *)&dctl->claimed;
-            while (c < av) {
-                const unsigned long long prev = atomicCAS(&dctl->claimed, c, c + 1);
-                if (prev == c) { kind = 1; unit = (long long)c; break; }
-                c = prev;
-            }
-            if (!kind && !ORDERED) {
+            // donated subtrees of requests in flight come before fresh
+            // requests: under load, fresh arrivals would otherwise keep every
+            // warp busy while a started request waits for its subtrees
+            if (!ORDERED) {
                 const int P = *(volatile int *)&pool->produced;
                 int C = *(volatile int *)&pool->consumed;
                 while (C < P) {
                     const int prev = atomicCAS(&pool->consumed, C, C + 1);
                     if (prev == C) { kind = 2; unit = C; break; }
                     C = prev;
+                }
+            }
+            if (!kind) {
+                const unsigned long long av = *(volatile unsigned long long *)&dctl->available;
+                unsigned long long c = *(volatile unsigned long long *)&dctl->claimed;
+                while (c < av) {
+                    const unsigned long long prev = atomicCAS(&dctl->claimed, c, c + 1);
+                    if (prev == c) { kind = 1; unit = (long long)c; break; }
+                    c = prev;
                 }
             }
             if (kind) atomicAdd(&pool->active, 1);  // counts holders only
@@ -175,7 +180,7 @@ __global__ void __launch_bounds__(256) td_serve_kernel(const td_instance *ring, 
                     atomicAdd(&dctl->served, 1ull);
                 }
             } else {
-                td_setup_root(s, x, code, codeN);
+                td_setup_root<ORDERED>(s, x, code, codeN);
                 run = true;
             }
         } else {
@@ -210,7 +215,7 @@ __global__ void __launch_bounds__(256) td_serve_kernel(const td_instance *ring, 
                 const unsigned slot = (unsigned)(req % ring_size);
                 const uint4 v = __ldcg(reinterpret_cast<const uint4 *>(&queue[slot]));
                 const td_instance x = *reinterpret_cast<const td_instance *>(&v);
-                td_setup_root(s, x, code, codeN);
+                td_setup_root<ORDERED>(s, x, code, codeN);
                 d0 = it.depth;
                 if (lane == 0) {
                     s.L[d0] = it.L;
@@ -358,12 +363,14 @@ TD_API int td_serve_open(int device, unsigned ring_size, unsigned flags, double 
     if (ordered)
         td_serve_kernel<true><<<grid, warps * 32, smem, sv->stream>>>(
             sv->d_ring, sv->d_res, sv->d_done, ring_size, sv->d_hctl, sv->d_ctl, sv->d_queue, sv->d_state,
-            sv->d_pool, sv->d_items, sv->d_ready, sv->item_capacity, g_steal_grain, g_split_level, g_check_every, 0,
+            sv->d_pool, sv->d_items, sv->d_ready, sv->item_capacity, g_serve_grain, g_serve_split_level,
+            g_serve_check_every, 0,
             limit_ns);
     else
         td_serve_kernel<false><<<grid, warps * 32, smem, sv->stream>>>(
             sv->d_ring, sv->d_res, sv->d_done, ring_size, sv->d_hctl, sv->d_ctl, sv->d_queue, sv->d_state,
-            sv->d_pool, sv->d_items, sv->d_ready, sv->item_capacity, g_steal_grain, g_split_level, g_check_every, 0,
+            sv->d_pool, sv->d_items, sv->d_ready, sv->item_capacity, g_serve_grain, g_serve_split_level,
+            g_serve_check_every, 0,
             limit_ns);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, __LINE__);
     *handle = sv;

@@ -18,6 +18,11 @@ struct Emu {
     uint8_t lut[4096];
     uint8_t pt[TD_MAX_N * TD_PT_STRIDE];
     uint32_t m1[TD_MAX_DEPTH + 1][32], m2[TD_MAX_DEPTH + 1][32];
+    // free order (bit-sliced): rows by caller position, masks, pair slots, outcome words
+    uint32_t S[32], G[32], P[32], O, F;
+    uint32_t pc[TD_MAX_ROUNDS][32];
+    uint32_t pw[TD_MAX_DEPTH + 1][TD_MAX_ROUNDS][32];
+    int rounds;
     uint64_t L[TD_MAX_DEPTH + 1];
     int off[TD_MAX_DEPTH + 1];
     uint16_t path[TD_MAX_DEPTH];
@@ -58,6 +63,109 @@ int prepare(Emu &e, uint64_t L, int off) {
         }
     }
     return odd;
+}
+
+// Rows of the bit-sliced evaluation, computed the way the kernel does: lane c
+// is caller position c, its cycle leader the smallest caller position on the
+// cycle, dist the omega steps to it.  Returns the number of odd cycles.
+int prepare_rows(Emu &e, uint64_t L, int off) {
+    const int N = e.N;
+    int B[TD_MAX_N], pos[TD_MAX_N], nxt[32], lead[32], dist[32], len[32];
+    for (int p = 0; p < N; ++p) {
+        B[p] = p ? (int)td_nib(L, p - 1) + 1 : 0;
+        pos[B[p]] = p;
+    }
+    for (int c = 0; c < 32; ++c) nxt[c] = c;
+    for (int c = 0; c < N; ++c) {
+        const int p = (c + off) % N;
+        const int q = p ? p - 1 : N - 1;
+        const int y = (B[q] + 1) % N;
+        nxt[c] = (pos[y] - off + N) % N;
+    }
+    for (int c = 0; c < 32; ++c) {
+        int m = c, x = nxt[c], l = 1;
+        while (x != c) { if (x < m) m = x; x = nxt[x]; ++l; }
+        lead[c] = m;
+        len[c] = l;
+        int d = 0;
+        x = c;
+        while (x != m) { x = nxt[x]; ++d; }
+        dist[c] = d;
+    }
+    const uint32_t ACT = (1u << N) - 1u;
+    e.O = e.F = 0;
+    int odd = 0;
+    for (int c = 0; c < N; ++c) {
+        if (len[c] & 1) e.O |= 1u << c;
+        if (len[c] == 1) e.F |= 1u << c;
+        odd += lead[c] == c && (len[c] & 1);
+    }
+    for (int c = 0; c < N; ++c) {
+        uint32_t S = 0, lt = 0, D0 = 0;
+        for (int q = 0; q < 32; ++q) {
+            if (lead[q] == lead[c]) S |= 1u << q;
+            if (dist[q] < dist[c]) lt |= 1u << q;
+            if (dist[q] & 1) D0 |= 1u << q;
+        }
+        S &= ACT;
+        const uint32_t lodd = 0u - (uint32_t)(len[c] & 1);
+        e.S[c] = S;
+        e.G[c] = S & lt;
+        e.P[c] = S & ((D0 ^ (0u - (uint32_t)(dist[c] & 1))) ^ (lodd & ~lt));
+    }
+    return odd;
+}
+
+// Bit-sliced evaluation of the node at `level`: fills the outcome words and
+// returns the found move (i | j<<5 | k<<10) or -1.
+int evaluate_rows(Emu &e, int level, int odd) {
+    const int D = level + 1;
+    const uint32_t f0 = 0u - ((e.acc[D] >> odd) & 1u), f2 = 0u - ((e.acc[D] >> (odd + 2)) & 1u);
+    const uint32_t x0 = (D < e.maxd ? 0u - ((e.reach[D] >> odd) & 1u) : 0u) & ~f0;
+    const uint32_t x2 = (D < e.maxd ? 0u - ((e.reach[D] >> (odd + 2)) & 1u) : 0u) & ~f2;
+    const uint32_t ACT = (1u << e.N) - 1u;
+    uint32_t best = 0xffffffffu;
+    for (int lane = 0; lane < 32; ++lane) {
+        uint32_t key = 0xffffffffu;
+        for (int r = 0; r < e.rounds; ++r) {
+            const uint32_t code = e.pc[r][lane];
+            const int i = code & 31, j = (code >> 5) & 31, ks = (code >> 10) & 31;
+            uint32_t plus, zero;
+            td_row_classes_x(e.S[i], e.G[i], e.P[i], e.S[j], e.G[j], e.P[j], e.O, e.F, 0u - ((e.O >> i) & 1u),
+                             0u - ((e.O >> j) & 1u), 0u - ((e.F >> i) & 1u), 0u - ((e.F >> j) & 1u), (int)(code >> 15),
+                             &plus, &zero);
+            const uint32_t km = ACT & (0xfffffffeu << ks);
+            const uint32_t fnd = km & ((f0 & zero) | (f2 & plus));
+            const uint32_t e2 = km & x2 & plus, e0 = km & x0 & zero;
+            e.pw[level][r][lane] = (e2 >> 1) | (e0 << 15);
+            if (fnd && key == 0xffffffffu)
+                key = ((uint32_t)lane << 17) | ((uint32_t)r << 15) | (code & 1023u) | ((uint32_t)(31 - __builtin_clz(fnd)) << 10);
+        }
+        if (key < best) best = key;
+    }
+    e.expansions++;
+    return best == 0xffffffffu ? -1 : (int)(best & 0x7fffu);
+}
+
+// Next child of `level` in the free order: +2 children first, the highest
+// pair slot R*lane + r (lexicographically smallest pair) and the smallest k.
+// Returns the move or -1.
+int next_child_rows(Emu &e, int level) {
+    bool any2 = false;
+    for (int lane = 0; lane < 32; ++lane)
+        for (int r = 0; r < e.rounds; ++r) any2 |= (e.pw[level][r][lane] & 0xffffu) != 0;
+    const uint32_t cm = any2 ? 0x0000ffffu : 0xffff0000u;
+    int best = -1;
+    for (int lane = 0; lane < 32; ++lane)
+        for (int r = 0; r < e.rounds; ++r)
+            if (e.pw[level][r][lane] & cm) best = e.rounds * lane + r;
+    if (best < 0) return -1;
+    const int lane = best / e.rounds, r = best % e.rounds;
+    const uint32_t w = e.pw[level][r][lane] & cm;
+    const int b = __builtin_ctz(w);
+    e.pw[level][r][lane] &= ~(1u << b);
+    const int k = any2 ? b + 1 : b - 15;
+    return (int)((e.pc[r][lane] & 1023u) | ((uint32_t)k << 10));
 }
 
 // Evaluate the children of the node at `level` (parent odd count `odd`).
@@ -136,7 +244,68 @@ int next_child(Emu &e, int level, int *accepted) {
     return 32 * s + lane;
 }
 
+int search_rows(Emu &e, td_result *res) {
+    const int NP = (e.N - 1) * (e.N - 2) / 2;
+    e.rounds = (NP + 31) / 32;
+    for (int r = 0; r < TD_MAX_ROUNDS; ++r)
+        for (int lane = 0; lane < 32; ++lane) e.pc[r][lane] = td_pair_code(e.N, r < e.rounds ? e.rounds * lane + r : -1);
+    int level = 0;
+    int odd = prepare_rows(e, e.L[0], e.off[0]);
+    int found = evaluate_rows(e, 0, odd);
+    for (;;) {
+        if (found >= 0) {
+            for (int d = 0; d < level; ++d) res->moves[d] = e.path[d];
+            res->moves[level] = (uint16_t)found;
+            res->depth = level + 1;
+            res->status = TD_FOUND;
+            break;
+        }
+        const int t = next_child_rows(e, level);
+        if (t < 0) {
+            if (level == 0) { res->status = TD_NOT_FOUND; break; }
+            --level;
+            continue;
+        }
+        e.path[level] = (uint16_t)t;
+        int noff;
+        td_apply_move(e.L[level], e.off[level], e.N, t & 31, (t >> 5) & 31, (t >> 10) & 31, &e.L[level + 1], &noff);
+        e.off[level + 1] = noff;
+        ++level;
+        odd = prepare_rows(e, e.L[level], e.off[level]);
+        found = evaluate_rows(e, level, odd);
+    }
+    res->expansions = e.expansions;
+    return res->status;
+}
+
 }  // namespace
+
+// Compares the bit-sliced classes of every triple of the state (L, off) with
+// the 12-bit class table; returns the number of triples that differ.
+extern "C" int td_emu_row_check(uint64_t L, int off, int N) {
+    static thread_local Emu e;
+    e.N = N;
+    prepare(e, L, off);
+    prepare_rows(e, L, off);
+    const uint32_t ACT = (1u << N) - 1u;
+    int bad = 0;
+    for (int i = 0; i < N; ++i)
+        for (int j = i + 1; j < N; ++j) {
+            uint32_t plus, zero;
+            td_row_classes(e.S[i], e.G[i], e.P[i], e.S[j], e.G[j], e.P[j], e.O, e.F, i, j, &plus, &zero);
+            plus &= ACT;
+            zero &= ACT;
+            for (int k = j + 1; k < N; ++k) {
+                const int idx = e.pt[i * TD_PT_STRIDE + j] | (e.pt[j * TD_PT_STRIDE + k] << 4) |
+                                (e.pt[k * TD_PT_STRIDE + i] << 8);
+                const int cls = td_class_of_index(idx);
+                const int got = ((plus >> k) & 1) ? TD_CLASS_PLUS2 : (((zero >> k) & 1) ? TD_CLASS_ZERO : TD_CLASS_SKIP);
+                if (((plus >> k) & 1) && ((zero >> k) & 1)) ++bad;
+                else if (got != cls) ++bad;
+            }
+        }
+    return bad;
+}
 
 extern "C" int td_emu_search(const td_instance *x, unsigned flags, td_result *res) {
     static thread_local Emu e;
@@ -164,6 +333,7 @@ extern "C" int td_emu_search(const td_instance *x, unsigned flags, td_result *re
     e.expansions = 0;
     e.L[0] = x->perm;
     e.off[0] = x->offset;
+    if (!e.ordered) return search_rows(e, res);
     int level = 0;
     int odd = prepare(e, e.L[0], e.off[0]);
     int found = evaluate(e, 0, odd);

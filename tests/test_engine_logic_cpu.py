@@ -1,6 +1,8 @@
 """The engine's warp algorithm, emulated one lane at a time on the host,
 against the oracle: identical witnesses and expansion counts in ordered mode,
-identical verdicts with replayable witnesses in free order."""
+identical verdicts with replayable witnesses in free order (bit-sliced
+classification), and the bit-sliced classes equal to the 12-bit class table on
+every triple."""
 import ctypes as C
 import random
 
@@ -75,6 +77,53 @@ def test_free_order_verdicts_and_replay(oracle, emu, seed):
         x = _prep(emu, beta, omega, init, 0.0, maxd, True)
         r, emv = _run(emu, x, 0)
         assert r.status == rc
+        if rc == 1:
+            abc = oracle.positions_to_symbols(beta, emv)
+            assert oracle.validate(beta, omega, abc, maxd) is None
+
+
+def test_bit_sliced_classes_match_class_table(emu):
+    """td_row_classes over all k of a pair equals td_class_of_index on the
+    pair-table entries of every triple, on random pinned states of S_2..S_16
+    with the caller's array starting anywhere."""
+    emu.td_emu_row_check.argtypes = [C.c_uint64, C.c_int, C.c_int]
+    rng = random.Random(9)
+    checked = 0
+    for _ in range(3000):
+        N = rng.randint(3, 17)
+        perm = list(range(N - 1))
+        rng.shuffle(perm)
+        if rng.random() < 0.2:  # near-identity states have many fixed points
+            perm = sorted(perm)
+            a, b = sorted(rng.sample(range(N - 1), 2)) if N > 2 else (0, 0)
+            perm[a], perm[b] = perm[b], perm[a]
+        L = 0
+        for m in range(16):
+            L |= (perm[m] if m < N - 1 else m) << (4 * m)
+        assert emu.td_emu_row_check(L, rng.randrange(N), N) == 0, (perm, N)
+        checked += 1
+    assert checked == 3000
+
+
+@pytest.mark.parametrize("seed", [6])
+def test_free_order_larger_instances(oracle, emu, seed):
+    """Free order on n = 10..13 (several pair slots per lane), bound
+    floor(n/2)+1 and one below it."""
+    rng = random.Random(seed)
+    for _ in range(24):
+        n = rng.randint(10, 13)
+        pi = list(range(n))
+        rng.shuffle(pi)
+        if rng.random() < 0.5:
+            pi = list(range(n))[::-1]
+            a, b = sorted(rng.sample(range(n), 2))
+            pi[a], pi[b] = pi[b], pi[a]
+        beta, omega, init = oracle.perm_to_pair(pi)
+        maxd = n // 2 + 1 - rng.randint(0, 1)
+        rc, _, _ = oracle.search(beta, omega, init, 0.0, maxd, True)
+        x = _prep(emu, beta, omega, init, 0.0, maxd, True)
+        r, emv = _run(emu, x, 0)
+        assert r.status == rc, (pi, maxd)
         if rc == 1:
             abc = oracle.positions_to_symbols(beta, emv)
             assert oracle.validate(beta, omega, abc, maxd) is None
