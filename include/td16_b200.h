@@ -213,9 +213,12 @@ int td_serve_open(int device, unsigned ring_size, unsigned flags,
                   double time_limit_s, void **handle, char *err, size_t errlen);
 int td_serve_workers(void *handle);
 /* TD_OVERFLOW while ring_size requests are unfinished */
+/* Publishes one request; *ticket numbers it.  Returns TD_OVERFLOW while the
+ * request's ring slot (ticket mod ring_size) still holds the result of the
+ * request ring_size tickets earlier that has not been taken by td_serve_poll. */
 int td_serve_submit(void *handle, const td_instance *instance,
                     unsigned long long *ticket);
-/* 1 (result copied) when done, else 0 */
+/* 1 (result copied; the slot may then be reused) when done, else 0 */
 int td_serve_poll(void *handle, unsigned long long ticket, td_result *out);
 int td_serve_close(void *handle, char *err, size_t errlen);
 

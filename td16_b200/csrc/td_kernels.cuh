@@ -664,7 +664,10 @@ __device__ __forceinline__ int td_donate(td_warp_smem &s, const td_donate_ctx &d
                 // wait until its taker has read it (bounded)
                 const uint32_t freed = td_ring_tag(slot - dc.capacity) | 0x80000000u;
                 for (unsigned spin = 0; *(volatile uint32_t *)&dc.ready[phys] != freed; ++spin) {
-                    if ((spin & 255u) == 0 && dc.deadline_ns && td_globaltimer() > dc.deadline_ns) break;
+                    if ((spin & 255u) == 0 && dc.deadline_ns && td_globaltimer() > dc.deadline_ns) {
+                        atomicCAS(&dc.pool->error, 0, TD_ERR_TIMEOUT);
+                        break;
+                    }
                     __nanosleep(64);
                 }
             }

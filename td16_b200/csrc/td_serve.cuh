@@ -24,7 +24,27 @@ struct td_serve_dev_ctl {      // device memory: scheduler state of the launch
     int stop;
     int error;
     unsigned long long served;
+    // where the first bounded wait gave up (1 dispatcher at the deadline,
+    // 2 a taker waiting for a donated item, 3 a donor waiting for a ring slot),
+    // the item index it waited for, and the pool counters at that moment
+    int where;
+    int snap_produced, snap_consumed, snap_active, snap_idle;
+    int pad;
+    long long index;
 };
+
+// Records the first wait that gave up (see td_serve_dev_ctl).
+__device__ __forceinline__ void td_serve_record(td_serve_dev_ctl *dctl, const td_pool *pool, int where,
+                                                long long index) {
+    if (atomicCAS(&dctl->where, 0, where) == 0) {
+        dctl->index = index;
+        dctl->snap_produced = *(volatile const int *)&pool->produced;
+        dctl->snap_consumed = *(volatile const int *)&pool->consumed;
+        dctl->snap_active = *(volatile const int *)&pool->active;
+        dctl->snap_idle = *(volatile const int *)&pool->idle;
+    }
+    atomicCAS(&dctl->error, 0, TD_ERR_TIMEOUT);
+}
 
 // Worker warps take fresh requests in arrival order and, in free order, also
 // donated subtrees of requests that others are searching (the batch engine's
@@ -70,7 +90,7 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
             }
             if (td_globaltimer() > deadline) {
                 if (lane == 0) {
-                    atomicCAS(&dctl->error, 0, TD_ERR_TIMEOUT);
+                    td_serve_record(dctl, pool, 1, -1);
                     atomicExch(&dctl->stop, 1);
                 }
                 break;
@@ -194,7 +214,7 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
                     if ((spin & 1023u) == 0 && td_globaltimer() > deadline) break;
                     __nanosleep(32);
                 }
-                if (!ok) atomicCAS(&dctl->error, 0, TD_ERR_TIMEOUT);
+                if (!ok) td_serve_record(dctl, pool, 2, unit);
                 __threadfence();
             }
             ok = __shfl_sync(TD_FULL, ok, 0);
@@ -275,6 +295,10 @@ struct Server {
     int item_capacity = 0;
     unsigned long long published = 0;
     int workers = 0;
+    // per slot: ticket + 1 of the last request whose result the client took
+    // (td_serve_poll); a slot is reused only after that, so a result stamp
+    // is never overwritten before the client has read it
+    std::vector<unsigned long long> taken;
 };
 
 void server_free(Server *sv) {
@@ -315,6 +339,7 @@ TD_API int td_serve_open(int device, unsigned ring_size, unsigned flags, double 
     sv->device = device;
     sv->flags = flags;
     sv->R = ring_size;
+    sv->taken.assign(ring_size, 0ull);
     auto fail = [&](cudaError_t e, int line) {
         set_err(err, errlen, cuda_msg(e, __FILE__, line));
         server_free(sv);
@@ -385,7 +410,7 @@ TD_API int td_serve_submit(void *handle, const td_instance *x, unsigned long lon
     auto *sv = static_cast<Server *>(handle);
     const unsigned long long r = sv->published;
     const unsigned slot = (unsigned)(r % sv->R);
-    if (r >= sv->R && __atomic_load_n(&sv->h_done[slot], __ATOMIC_ACQUIRE) != r - sv->R + 1) return TD_OVERFLOW;
+    if (r >= sv->R && __atomic_load_n(&sv->taken[slot], __ATOMIC_ACQUIRE) != r - sv->R + 1) return TD_OVERFLOW;
     sv->h_ring[slot] = *x;
     __atomic_store_n(&sv->h_done[slot], 0ull, __ATOMIC_RELAXED);
     __atomic_thread_fence(__ATOMIC_SEQ_CST);
@@ -401,6 +426,7 @@ TD_API int td_serve_poll(void *handle, unsigned long long ticket, td_result *out
     const unsigned slot = (unsigned)(ticket % sv->R);
     if (__atomic_load_n(&sv->h_done[slot], __ATOMIC_ACQUIRE) != ticket + 1) return 0;
     if (out) std::memcpy(out, (const void *)&sv->h_res[slot], sizeof(td_result));
+    __atomic_store_n(&sv->taken[slot], ticket + 1, __ATOMIC_RELEASE);
     return 1;
 }
 
@@ -413,15 +439,24 @@ TD_API int td_serve_close(void *handle, char *err, size_t errlen) {
     cudaSetDevice(sv->device);
     cudaError_t e = cudaStreamSynchronize(sv->stream);
     td_serve_dev_ctl ctl;
+    td_pool pool;
     std::memset(&ctl, 0, sizeof ctl);
+    std::memset(&pool, 0, sizeof pool);
     if (e == cudaSuccess) e = cudaMemcpy(&ctl, sv->d_ctl, sizeof ctl, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&pool, sv->d_pool, sizeof pool, cudaMemcpyDeviceToHost);
     server_free(sv);
     if (e != cudaSuccess) {
         set_err(err, errlen, cuda_msg(e, __FILE__, __LINE__));
         return TD_CUDA_ERROR;
     }
-    if (ctl.error) {
-        set_err(err, errlen, "serving launch deadline reached");
+    if (ctl.error || pool.error) {
+        char msg[320];
+        std::snprintf(msg, sizeof msg,
+                      "serving launch deadline reached (wait %d, item %lld; produced %d consumed %d active %d "
+                      "idle %d; requests available %llu claimed %llu served %llu; donor ring wait %s)",
+                      ctl.where, ctl.index, ctl.snap_produced, ctl.snap_consumed, ctl.snap_active, ctl.snap_idle,
+                      ctl.available, ctl.claimed, ctl.served, pool.error ? "expired" : "ok");
+        set_err(err, errlen, msg);
         return TD_TIMEOUT;
     }
     return TD_OK;

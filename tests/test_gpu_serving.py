@@ -72,3 +72,38 @@ def test_admission_respects_the_pool(td):
     res, st = td._lib.serve_open_loop(0, inst, 50000.0, seed=4, pool_bytes=4000)
     assert st["served"] == 1000 and st["admission_wait_ms_mean"] > 0
     assert (res["status"] >= 0).all()
+
+
+def test_ring_slot_is_reused_only_after_its_result_is_taken(td):
+    """A request's ring slot holds its result until the client polls it: with a
+    ring of 8, the ninth submission waits for ticket 0 to be taken, even when
+    the device finished it long ago."""
+    perms, n, inst = _requests(td, 40, seed=5, n_max=12)
+    srv = td._lib.Server(0, 8, 0, 60.0)
+    try:
+        tickets = [srv.submit(x) for x in inst[:8]]
+        time.sleep(0.5)  # every one of them is done on the device by now
+        with pytest.raises(td.TdError):
+            srv.submit(inst[8])
+        first = None
+        deadline = time.time() + 30
+        while first is None and time.time() < deadline:
+            first = srv.poll(tickets[0])
+        assert first is not None
+        tickets.append(srv.submit(inst[8]))
+        results = [first]
+        for t in tickets[1:]:
+            r = None
+            deadline = time.time() + 30
+            while r is None and time.time() < deadline:
+                r = srv.poll(t)
+            assert r is not None
+            results.append(r)
+    finally:
+        srv.close()
+    td.init_slots(1, [0], 64 << 20)
+    try:
+        batch, _ = td.search_batch(0, inst[:9], 0)
+    finally:
+        td.destroy()
+    assert [int(r["status"]) for r in results] == [int(s) for s in batch["status"]]
