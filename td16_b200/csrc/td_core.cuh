@@ -190,7 +190,7 @@ TD_HD int td_class_of_index(int idx) {
 TD_HD void td_row_classes_x(uint32_t Si, uint32_t Gi, uint32_t Pi, uint32_t Sj, uint32_t Gj, uint32_t Pj,
                             uint32_t O, uint32_t F, uint32_t oi, uint32_t oj, uint32_t fi, uint32_t fj, int sh,
                             uint32_t *plus2, uint32_t *zero) {
-    const uint32_t s1 = (uint32_t)((int32_t)(Si << sh) >> 31);   // i and j on one cycle
+    const uint32_t s1 = Si == Sj ? 0xffffffffu : 0u;             // i and j on one cycle (equal rows)
     const uint32_t p1 = (uint32_t)((int32_t)(Pi << sh) >> 31);   // walk i -> j odd
     const uint32_t g1 = (uint32_t)((int32_t)(Gi << sh) >> 31);   // dist(i) > dist(j)
     const uint32_t P3 = Pi ^ oi;                 // walk k -> i odd (k on i's cycle)
@@ -223,11 +223,14 @@ TD_HD void td_row_classes(uint32_t Si, uint32_t Gi, uint32_t Pi, uint32_t Sj, ui
 // first two positions of a triple), numbered so that higher slots hold
 // lexicographically smaller pairs.  Returns i | j << 5 | j << 10 | (31-j) << 15
 // (the third field is the shift of the k mask, k > j; the fourth brings bit j
-// to the sign bit), or 0 | 1 << 5 | 31 << 10 | 30 << 15 for a slot past the
-// last pair (an empty k mask).
+// to the sign bit).  A slot past the last pair, or a negative one, gets
+// i = 0, j = N-1: no position lies after N-1, so its k mask is empty.
 TD_HD uint32_t td_pair_code(int N, int q) {
     const int NP = N < 3 ? 0 : (N - 1) * (N - 2) / 2;
-    if (q < 0 || q >= NP) return (1u << 5) | (31u << 10) | (30u << 15);
+    if (q < 0 || q >= NP) {
+        const uint32_t jj = N >= 2 ? (uint32_t)(N - 1) : 0u;
+        return (jj << 5) | (jj << 10) | ((31u - jj) << 15);
+    }
     int rank = NP - 1 - q;  // lexicographic rank of the pair
     int i = 0;
     while (rank >= N - 2 - i) {  // pairs with first element i: j = i+1 .. N-2

@@ -38,7 +38,10 @@ struct td_warp_smem {
             uint32_t pm[TD_MAX_DEPTH][3][32];
         };
         struct {  // free move order (bit-sliced: one pair and all its k per lane and round)
-            uint4 rows[TD_MAX_N];                      // per caller position: S, G, P row masks
+            // per caller position c: the row masks S, G, P and H (positions
+            // after c), and the odd-cycle / fixed-point flags as full masks
+            uint4 rows[TD_MAX_N];
+            uint2 flg[TD_MAX_N];
             // per level and lane: the expandable children of the lane's four
             // pair slots (word r = slot 4*lane + r), +2 class at bits k-1
             // (1..15), 0 class at bits k+15 (17..31)
@@ -418,9 +421,10 @@ __device__ __forceinline__ int td_prepare_rows(td_warp_smem &s, int level, int N
     O = __ballot_sync(TD_FULL, act && (len & 1));
     F = __ballot_sync(TD_FULL, act && len == 1);
     const int odd = __popc(__ballot_sync(TD_FULL, act && m == c && (len & 1)));
-    // fourth word: byte 0 = 0xff when c's cycle is odd, byte 1 = 0xff when c is fixed
-    const uint32_t flags = ((len & 1) ? 0x00ffu : 0u) | (len == 1 ? 0xff00u : 0u);
-    if (act) s.rows[c] = make_uint4(S, G, P, flags);
+    if (act) {
+        s.rows[c] = make_uint4(S, G, P, ACT & (0xfffffffeu << c));
+        s.flg[c] = make_uint2(lodd, len == 1 ? 0xffffffffu : 0u);
+    }
     __syncwarp();
     return odd;
 }
@@ -444,14 +448,16 @@ __device__ __forceinline__ int td_evaluate_rows(td_warp_smem &s, const uint32_t 
     for (int r = 0; r < TD_MAX_ROUNDS; ++r) {
         if (r >= R) break;
         const uint32_t pc = code[r];
-        const int i = pc & 31, j = (pc >> 5) & 31, ks = (pc >> 10) & 31;
+        const int i = pc & 31, j = (pc >> 5) & 31;
         const uint4 ri = s.rows[i], rj = s.rows[j];
+        const uint2 fi = s.flg[i], fj = s.flg[j];
         uint32_t plus, zero;
-        td_row_classes_x(ri.x, ri.y, ri.z, rj.x, rj.y, rj.z, O, F, __byte_perm(ri.w, 0, 0x0000),
-                         __byte_perm(rj.w, 0, 0x0000), __byte_perm(ri.w, 0, 0x1111), __byte_perm(rj.w, 0, 0x1111),
-                         (int)(pc >> 15), &plus, &zero);
-        const uint32_t km = ACT & (0xfffffffeu << ks);
-        W[r] = ((km & x2 & plus) >> 1) | ((km & x0 & zero) << 15);
+        td_row_classes_x(ri.x, ri.y, ri.z, rj.x, rj.y, rj.z, O, F, fi.x, fj.x, fi.y, fj.y, (int)(pc >> 15), &plus,
+                         &zero);
+        const uint32_t km = rj.w;  // k > j (empty slots: j's row with an empty mask is never read)
+        // +2 children at bits k-1, 0 children at bits k+15; the fields do not
+        // overlap, so the high-half multiply and the add keep this off the ALU pipe
+        W[r] = __umulhi(km & x2 & plus, 0x80000000u) + (km & x0 & zero) * 32768u;
         if (accepting) {
             const uint32_t fnd = km & ((f0 & zero) | (f2 & plus));
             if (fnd && key == 0xffffffffu)
