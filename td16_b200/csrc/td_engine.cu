@@ -53,6 +53,7 @@ static_assert(sizeof(td_result) == 32, "td_result layout");
 // ============================================================================
 
 #define TD_LUT_BYTES 4096
+#define TD_TT_BITS 10  // 1024 explored-state entries (8 KiB) per warp of a free-order launch
 
 // Class table (td_class_of_index for every 12-bit index), filled by the host.
 __device__ __align__(16) uint8_t td_lut_global[TD_LUT_BYTES];
@@ -72,6 +73,8 @@ __device__ __forceinline__ td_search_limits td_make_limits(uint64_t max_exp, uin
     lim.max_expansions = max_exp ? max_exp : ~0ull;
     lim.deadline_ns = time_limit_ns ? td_globaltimer() + time_limit_ns : 0;
     lim.abort_flag = abort_flag;
+    lim.tt = nullptr;
+    lim.tt_bits = 0;
     return lim;
 }
 
@@ -168,7 +171,8 @@ __global__ void __launch_bounds__(256, 4) td_steal_kernel(const td_instance *__r
                                                       td_result *__restrict__ out, int count, td_pool *pool,
                                                       td_item *items, uint32_t *ready, const uint32_t *epoch_ptr,
                                                       int capacity, td_inst_state *state, int grain,
-                                                      int max_level, int check_every, uint64_t time_limit_ns) {
+                                                      int max_level, int check_every, uint64_t time_limit_ns,
+                                                      uint64_t *tt, int tt_bits) {
     extern __shared__ __align__(16) uint8_t td_smem[];
     const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint8_t *lut = td_smem;
@@ -178,6 +182,10 @@ __global__ void __launch_bounds__(256, 4) td_steal_kernel(const td_instance *__r
     uint32_t code[TD_MAX_STEPS];
     int codeN = -1;
     td_search_limits lim = td_make_limits(0, time_limit_ns, nullptr);
+    if (tt) {
+        lim.tt = tt + ((size_t)(blockIdx.x * warps + warp) << tt_bits);
+        lim.tt_bits = tt_bits;
+    }
     td_donate_ctx dc;
     dc.pool = pool;
     dc.items = items;
@@ -398,6 +406,8 @@ struct Slot {
     td_item *d_items = nullptr;
     uint32_t *d_ready = nullptr;
     int item_capacity = 0;
+    uint64_t *d_tt = nullptr;  // tables of explored states, one per resident warp
+    size_t tt_warps = 0;
     td_inst_state *d_state = nullptr;
     size_t state_count = 0;
     uint32_t *d_epoch = nullptr;
@@ -500,6 +510,7 @@ void release_slot(Slot &s) {
     if (s.d_pool) cudaFree(s.d_pool);
     if (s.d_items) cudaFree(s.d_items);
     if (s.d_ready) cudaFree(s.d_ready);
+    if (s.d_tt) cudaFree(s.d_tt);
     if (s.d_epoch) cudaFree(s.d_epoch);
     if (s.d_state) cudaFree(s.d_state);
     if (s.h_inst) cudaFreeHost(s.h_inst);
@@ -560,12 +571,23 @@ int launch_batch(Slot &s, int count, const td_instance *d_in, td_result *d_out, 
         const int resident = d.sms * d.steal_blocks_per_sm;
         const int share = std::max(1, resident / std::max(1, s.slots_on_device));
         const int grid = std::max(1, std::min(resident, std::max(share, (count + warps - 1) / warps)));
+        if ((size_t)resident * warps > s.tt_warps) {
+            // one table (8 bytes x 2^TD_TT_BITS) per resident warp, sized for
+            // the whole resident grid so that it never moves under a captured
+            // graph; the launch waits for the previous one before replacing it
+            TD_CHECK(cudaStreamSynchronize(stream));
+            if (s.d_tt) TD_CHECK(cudaFree(s.d_tt));
+            s.d_tt = nullptr;
+            s.tt_warps = 0;
+            TD_CHECK(cudaMalloc(&s.d_tt, ((size_t)resident * warps << TD_TT_BITS) * sizeof(uint64_t)));
+            s.tt_warps = (size_t)resident * warps;
+        }
         TD_CHECK(cudaMemsetAsync(s.d_pool, 0, sizeof(td_pool), stream));
         TD_CHECK(cudaMemsetAsync(s.d_state, 0, (size_t)count * sizeof(td_inst_state), stream));
         td_epoch_kernel<<<1, 1, 0, stream>>>(s.d_epoch);
         td_steal_kernel<<<grid, threads, smem, stream>>>(d_in, d_out, count, s.d_pool, s.d_items, s.d_ready, s.d_epoch,
                                                          s.item_capacity, s.d_state, g_steal_grain, g_split_level,
-                                                         g_check_every, time_limit_ns());
+                                                         g_check_every, time_limit_ns(), s.d_tt, TD_TT_BITS);
     } else {
         DeviceInfo &d = g_dev[s.device];
         if (d.blocks_per_sm == 0) {
@@ -1248,7 +1270,7 @@ TD_API int td_search_batch_noalloc(int count, const td_instance *d_instances, td
         const int grid = std::max(1, std::min(d.sms * std::max(1, d.steal_blocks), blocks_needed));
         td_steal_kernel<<<grid, threads, smem, st>>>(d_instances, d_results, count, pool, items, ready, epoch,
                                                      TD_NOALLOC_ITEMS, state, g_steal_grain, g_split_level,
-                                                     g_check_every, limit);
+                                                     g_check_every, limit, nullptr, 0);
     }
     TD_CHECK_NA(cudaGetLastError());
     if (flags & TD_FLAG_VERIFY) {

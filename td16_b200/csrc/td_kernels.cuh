@@ -205,6 +205,8 @@ struct td_search_limits {
     uint64_t max_expansions;   // per search; TD_ERR_BUDGET when exceeded
     uint64_t deadline_ns;      // %globaltimer value; 0 = none
     const int *abort_flag;     // optional host/device abort request
+    uint64_t *tt;              // this warp's table of explored states (free order); null = none
+    int tt_bits;               // log2 of its entries
 };
 
 __device__ __forceinline__ uint64_t td_globaltimer() {
@@ -439,7 +441,6 @@ __device__ __forceinline__ int td_evaluate_rows(td_warp_smem &s, const uint32_t 
     const uint32_t f0 = 0u - ((accD >> odd) & 1u), f2 = 0u - ((accD >> (odd + 2)) & 1u);
     const uint32_t x0 = (0u - ((reachD >> odd) & 1u)) & ~f0;
     const uint32_t x2 = (0u - ((reachD >> (odd + 2)) & 1u)) & ~f2;
-    const uint32_t ACT = (1u << N) - 1u;
     const bool accepting = (f0 | f2) != 0;  // warp-uniform
     const int R = (int)code[TD_MAX_ROUNDS];  // warp-uniform
     uint32_t key = 0xffffffffu;
@@ -695,6 +696,64 @@ __device__ __forceinline__ int td_donate(td_warp_smem &s, const td_donate_ctx &d
     return give;
 }
 
+// ---- table of explored states (free order) --------------------------------
+//
+// Different move orders reach the same state: on near-reverse S_16 about 80%
+// of the free-order expansions re-expand a state already expanded at the same
+// or a smaller depth.  Whether a node's subtree holds a witness depends only
+// on its pinned state L (not on where the caller's array starts: a move is the
+// same cycle rotation from any start, so the reachable states do not depend
+// on it) and on its depth.  Each warp keeps a direct-mapped table of
+// (L, depth) for the states it expanded in its current unit, and skips a
+// child whose state is in the table at a depth <= the child's.  This is sound:
+// the earlier node was explored with at least as much budget, unless it is an
+// ancestor still being explored (which has more budget) or its children were
+// donated (then their takers explore them).  The search stops at the first
+// witness, so every completed entry is a state without one.  An entry is one
+// word: the low 15 nibbles of L (the 16th is the missing value of the
+// permutation) and the depth in the top nibble.  The table is cleared at the
+// start of each unit, since the rate masks and the bound belong to the
+// instance.
+
+#define TD_TT_EMPTY 0xffffffffffffffffull  // no state has fifteen nibbles of 15
+#define TD_TT_LOW60 0x0fffffffffffffffull
+
+__device__ __forceinline__ void td_tt_clear(const td_search_limits &lim) {
+    const int lane = threadIdx.x & 31;
+    uint4 *t = reinterpret_cast<uint4 *>(lim.tt);
+    const int n4 = 1 << (lim.tt_bits - 1);
+    for (int q = lane; q < n4; q += 32) t[q] = make_uint4(~0u, ~0u, ~0u, ~0u);
+    __syncwarp();
+}
+
+// Looks up the state of level `lv` (depth lv) and records it; returns whether
+// it was already explored at a depth <= lv (uniform across the warp).
+__device__ __forceinline__ bool td_tt_visit(const td_warp_smem &s, const td_search_limits &lim, int lv, int N) {
+    const int m = threadIdx.x & 31;
+    const int a = m < N ? s.A[lv][m] : 0xff;
+    const int c0 = __ffs(__ballot_sync(TD_FULL, a == 0)) - 1;  // caller position of label 0
+    // L[m] = A[(m + 1 + c0) mod N] - 1 for m < N - 1
+    int src = m + 1 + c0;
+    src -= src >= N ? N : 0;
+    const int v = __shfl_sync(TD_FULL, a, m < N - 1 ? src : m) - 1;
+    uint32_t lo = 0, hi = 0;
+    if (m < N - 1) {
+        if (m < 8) lo = (uint32_t)v << (4 * m);
+        else hi = (uint32_t)v << (4 * (m - 8));
+    }
+    lo = __reduce_or_sync(TD_FULL, lo);
+    hi = __reduce_or_sync(TD_FULL, hi);
+    const uint64_t key = ((((uint64_t)hi) << 32) | lo) & TD_TT_LOW60;
+    int hit = 0;
+    if (m == 0) {
+        const uint32_t h = (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> (64 - lim.tt_bits));
+        const uint64_t old = lim.tt[h];
+        hit = (old & TD_TT_LOW60) == key && (int)(old >> 60) <= lv;
+        if (!hit) lim.tt[h] = key | ((uint64_t)lv << 60);
+    }
+    return __shfl_sync(TD_FULL, hit, 0) != 0;
+}
+
 // Depth-first search from the node held at level d0 of `s` (state, path and
 // rate masks already set).  Leaves the frames intact on TD_DFS_BUDGET.  The
 // reference order evaluates one triple per lane and step (`code` holds the
@@ -721,6 +780,10 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
         if (found >= 0) found = td_tri_table[tri_base + T - 1 - found];
     } else {
         td_unpack_state(s, d0, s.L[d0], s.off[d0], N);
+        if (lim.tt) {
+            td_tt_clear(lim);
+            (void)td_tt_visit(s, lim, d0, N);
+        }
         const int odd = td_prepare_rows(s, d0, N, O, F);
         found = td_evaluate_rows(s, code, N, d0, odd, O, F);
     }
@@ -811,6 +874,7 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
         } else {
             if (lane == 0) s.path[level] = (uint16_t)t;
             td_apply_bytes(s, level, t, N);
+            if (lim.tt && td_tt_visit(s, lim, level + 1, N)) continue;  // explored with at least this budget
             ++level;
             const int odd = td_prepare_rows(s, level, N, O, F);
             found = td_evaluate_rows(s, code, N, level, odd, O, F);

@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
                                                       td_instance *queue, td_inst_state *state, td_pool *pool,
                                                       td_item *items, uint32_t *ready, int item_capacity,
                                                       int grain, int max_level, int check_every, uint64_t max_exp,
-                                                      uint64_t time_limit_ns) {
+                                                      uint64_t time_limit_ns, uint64_t *tt, int tt_bits) {
     extern __shared__ __align__(16) uint8_t td_smem[];
     const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint8_t *lut = td_smem;
@@ -107,6 +107,8 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
     lim.max_expansions = max_exp ? max_exp : ~0ull;
     lim.deadline_ns = deadline;
     lim.abort_flag = nullptr;
+    lim.tt = (!ORDERED && tt) ? tt + ((size_t)(blockIdx.x * warps + warp) << tt_bits) : nullptr;
+    lim.tt_bits = tt_bits;
     td_donate_ctx dc;
     dc.ring = 1;
     dc.deadline_ns = deadline;
@@ -293,6 +295,7 @@ struct Server {
     td_item *d_items = nullptr;
     uint32_t *d_ready = nullptr;
     int item_capacity = 0;
+    uint64_t *d_tt = nullptr;  // tables of explored states, one per worker warp (free order)
     unsigned long long published = 0;
     int workers = 0;
     // per slot: ticket + 1 of the last request whose result the client took
@@ -315,6 +318,7 @@ void server_free(Server *sv) {
     if (sv->d_pool) cudaFree(sv->d_pool);
     if (sv->d_items) cudaFree(sv->d_items);
     if (sv->d_ready) cudaFree(sv->d_ready);
+    if (sv->d_tt) cudaFree(sv->d_tt);
     if (sv->stream) cudaStreamDestroy(sv->stream);
     delete sv;
 }
@@ -384,19 +388,21 @@ TD_API int td_serve_open(int device, unsigned ring_size, unsigned flags, double 
     }
     const int grid = g_dev[device].sms * std::max(1, per_sm);
     sv->workers = grid * warps - 1;
+    if (!ordered) {
+        const size_t tt_bytes = ((size_t)grid * warps << TD_TT_BITS) * sizeof(uint64_t);
+        if ((e = cudaMalloc(&sv->d_tt, tt_bytes)) != cudaSuccess) return fail(e, __LINE__);
+    }
     const uint64_t limit_ns = (uint64_t)((time_limit_s > 0 ? time_limit_s : 60.0) * 1e9);
     if (ordered)
         td_serve_kernel<true><<<grid, warps * 32, smem, sv->stream>>>(
             sv->d_ring, sv->d_res, sv->d_done, ring_size, sv->d_hctl, sv->d_ctl, sv->d_queue, sv->d_state,
             sv->d_pool, sv->d_items, sv->d_ready, sv->item_capacity, g_serve_grain, g_serve_split_level,
-            g_serve_check_every, 0,
-            limit_ns);
+            g_serve_check_every, 0, limit_ns, nullptr, 0);
     else
         td_serve_kernel<false><<<grid, warps * 32, smem, sv->stream>>>(
             sv->d_ring, sv->d_res, sv->d_done, ring_size, sv->d_hctl, sv->d_ctl, sv->d_queue, sv->d_state,
             sv->d_pool, sv->d_items, sv->d_ready, sv->item_capacity, g_serve_grain, g_serve_split_level,
-            g_serve_check_every, 0,
-            limit_ns);
+            g_serve_check_every, 0, limit_ns, sv->d_tt, TD_TT_BITS);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, __LINE__);
     *handle = sv;
     return TD_OK;

@@ -244,7 +244,24 @@ int next_child(Emu &e, int level, int *accepted) {
     return 32 * s + lane;
 }
 
+// The kernel's table of explored states (free order): 2^10 entries, key =
+// the low 15 nibbles of the pinned state (nibbles from N-1 on cleared), depth
+// in the top nibble, direct-mapped by a multiplicative hash.
+#define EMU_TT_BITS 10
+bool tt_visit(uint64_t *tt, uint64_t L, int N, int lv) {
+    const uint64_t data = N - 1 >= 16 ? ~0ull : ((1ull << (4 * (N - 1))) - 1ull);
+    const uint64_t key = L & data & 0x0fffffffffffffffull;
+    const unsigned h = (unsigned)((key * 0x9E3779B97F4A7C15ull) >> (64 - EMU_TT_BITS));
+    const uint64_t old = tt[h];
+    if ((old & 0x0fffffffffffffffull) == key && (int)(old >> 60) <= lv) return true;
+    tt[h] = key | ((uint64_t)lv << 60);
+    return false;
+}
+
 int search_rows(Emu &e, td_result *res) {
+    static thread_local uint64_t tt[1 << EMU_TT_BITS];
+    for (int q = 0; q < (1 << EMU_TT_BITS); ++q) tt[q] = ~0ull;
+    tt_visit(tt, e.L[0], e.N, 0);
     const int NP = (e.N - 1) * (e.N - 2) / 2;
     e.rounds = (NP + 31) / 32;
     for (int r = 0; r < TD_MAX_ROUNDS; ++r)
@@ -270,6 +287,7 @@ int search_rows(Emu &e, td_result *res) {
         int noff;
         td_apply_move(e.L[level], e.off[level], e.N, t & 31, (t >> 5) & 31, (t >> 10) & 31, &e.L[level + 1], &noff);
         e.off[level + 1] = noff;
+        if (tt_visit(tt, e.L[level + 1], e.N, level + 1)) continue;  // explored with at least this budget
         ++level;
         odd = prepare_rows(e, e.L[level], e.off[level]);
         found = evaluate_rows(e, level, odd);
