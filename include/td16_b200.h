@@ -124,6 +124,11 @@ int td_configure_steal(int grain, int split_level, int check_every);
 /* The same for later serving launches (td_serve_open), kept apart because a
  * serving launch trades throughput for latency (default 1, 2, 32). */
 int td_configure_serve(int grain, int split_level, int check_every);
+/* Free order only: each warp keeps a table of the states it explored in its
+ * current search and skips a child already explored with at least its depth
+ * budget.  2^bits entries of 8 bytes per resident warp (6..16; default 12),
+ * or 0 for none.  Verdicts do not depend on it. */
+int td_configure_table(int bits);
 
 /* ---- instance preparation (host, no GPU needed) -------------------------- */
 

@@ -30,7 +30,7 @@ GRID = {
     "warps": [4, 8],
     "grain": [1, 2, 4],
     "split_level": [2, 3, 4],
-    "check_every": [64, 256, 1024],
+    "check_every": [64, 256, 512, 1024],
 }
 QUICK = {"warps": [2, 4], "grain": [4, 8], "split_level": [4], "check_every": [32, 128]}
 

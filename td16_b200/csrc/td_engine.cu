@@ -53,7 +53,7 @@ static_assert(sizeof(td_result) == 32, "td_result layout");
 // ============================================================================
 
 #define TD_LUT_BYTES 4096
-#define TD_TT_BITS 10  // 1024 explored-state entries (8 KiB) per warp of a free-order launch
+#define TD_TT_BITS 12  // default: 4096 explored-state entries (32 KiB) per warp of a free-order launch
 
 // Class table (td_class_of_index for every 12-bit index), filled by the host.
 __device__ __align__(16) uint8_t td_lut_global[TD_LUT_BYTES];
@@ -408,6 +408,7 @@ struct Slot {
     int item_capacity = 0;
     uint64_t *d_tt = nullptr;  // tables of explored states, one per resident warp
     size_t tt_warps = 0;
+    int tt_bits = 0;
     td_inst_state *d_state = nullptr;
     size_t state_count = 0;
     uint32_t *d_epoch = nullptr;
@@ -435,6 +436,7 @@ int g_check_every = 8;      // expansions between idle checks
 int g_serve_grain = 1;
 int g_serve_split_level = 2;
 int g_serve_check_every = 32;
+int g_tt_bits = TD_TT_BITS;  // log2 entries of the explored-state tables; 0 = no table
 
 void set_err(char *err, size_t len, const std::string &msg) {
     if (err && len) {
@@ -571,7 +573,7 @@ int launch_batch(Slot &s, int count, const td_instance *d_in, td_result *d_out, 
         const int resident = d.sms * d.steal_blocks_per_sm;
         const int share = std::max(1, resident / std::max(1, s.slots_on_device));
         const int grid = std::max(1, std::min(resident, std::max(share, (count + warps - 1) / warps)));
-        if ((size_t)resident * warps > s.tt_warps) {
+        if (g_tt_bits > 0 && ((size_t)resident * warps > s.tt_warps || g_tt_bits != s.tt_bits)) {
             // one table (8 bytes x 2^TD_TT_BITS) per resident warp, sized for
             // the whole resident grid so that it never moves under a captured
             // graph; the launch waits for the previous one before replacing it
@@ -579,15 +581,17 @@ int launch_batch(Slot &s, int count, const td_instance *d_in, td_result *d_out, 
             if (s.d_tt) TD_CHECK(cudaFree(s.d_tt));
             s.d_tt = nullptr;
             s.tt_warps = 0;
-            TD_CHECK(cudaMalloc(&s.d_tt, ((size_t)resident * warps << TD_TT_BITS) * sizeof(uint64_t)));
+            TD_CHECK(cudaMalloc(&s.d_tt, ((size_t)resident * warps << g_tt_bits) * sizeof(uint64_t)));
             s.tt_warps = (size_t)resident * warps;
+            s.tt_bits = g_tt_bits;
         }
         TD_CHECK(cudaMemsetAsync(s.d_pool, 0, sizeof(td_pool), stream));
         TD_CHECK(cudaMemsetAsync(s.d_state, 0, (size_t)count * sizeof(td_inst_state), stream));
         td_epoch_kernel<<<1, 1, 0, stream>>>(s.d_epoch);
         td_steal_kernel<<<grid, threads, smem, stream>>>(d_in, d_out, count, s.d_pool, s.d_items, s.d_ready, s.d_epoch,
                                                          s.item_capacity, s.d_state, g_steal_grain, g_split_level,
-                                                         g_check_every, time_limit_ns(), s.d_tt, TD_TT_BITS);
+                                                         g_check_every, time_limit_ns(), g_tt_bits > 0 ? s.d_tt : nullptr,
+                                                         g_tt_bits);
     } else {
         DeviceInfo &d = g_dev[s.device];
         if (d.blocks_per_sm == 0) {
@@ -870,6 +874,16 @@ TD_API int td_configure_steal(int grain, int split_level, int check_every) {
     g_steal_grain = grain;
     g_split_level = split_level;
     g_check_every = check_every;
+    return TD_OK;
+}
+
+// Size of the per-warp tables of explored states of later free-order launches:
+// 2^bits entries of 8 bytes per resident warp (6 <= bits <= 16), or 0 to
+// search without them.
+TD_API int td_configure_table(int bits) {
+    if (bits != 0 && (bits < 6 || bits > 16)) return TD_INVALID_ARG;
+    std::lock_guard<std::mutex> g(g_mu);
+    g_tt_bits = bits;
     return TD_OK;
 }
 

@@ -388,8 +388,9 @@ TD_API int td_serve_open(int device, unsigned ring_size, unsigned flags, double 
     }
     const int grid = g_dev[device].sms * std::max(1, per_sm);
     sv->workers = grid * warps - 1;
-    if (!ordered) {
-        const size_t tt_bytes = ((size_t)grid * warps << TD_TT_BITS) * sizeof(uint64_t);
+    const int tt_bits = ordered ? 0 : g_tt_bits;
+    if (tt_bits > 0) {
+        const size_t tt_bytes = ((size_t)grid * warps << tt_bits) * sizeof(uint64_t);
         if ((e = cudaMalloc(&sv->d_tt, tt_bytes)) != cudaSuccess) return fail(e, __LINE__);
     }
     const uint64_t limit_ns = (uint64_t)((time_limit_s > 0 ? time_limit_s : 60.0) * 1e9);
@@ -402,7 +403,7 @@ TD_API int td_serve_open(int device, unsigned ring_size, unsigned flags, double 
         td_serve_kernel<false><<<grid, warps * 32, smem, sv->stream>>>(
             sv->d_ring, sv->d_res, sv->d_done, ring_size, sv->d_hctl, sv->d_ctl, sv->d_queue, sv->d_state,
             sv->d_pool, sv->d_items, sv->d_ready, sv->item_capacity, g_serve_grain, g_serve_split_level,
-            g_serve_check_every, 0, limit_ns, sv->d_tt, TD_TT_BITS);
+            g_serve_check_every, 0, limit_ns, sv->d_tt, tt_bits);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, __LINE__);
     *handle = sv;
     return TD_OK;

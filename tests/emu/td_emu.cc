@@ -244,10 +244,10 @@ int next_child(Emu &e, int level, int *accepted) {
     return 32 * s + lane;
 }
 
-// The kernel's table of explored states (free order): 2^10 entries, key =
+// The kernel's table of explored states (free order): 2^12 entries, key =
 // the low 15 nibbles of the pinned state (nibbles from N-1 on cleared), depth
 // in the top nibble, direct-mapped by a multiplicative hash.
-#define EMU_TT_BITS 10
+#define EMU_TT_BITS 12
 bool tt_visit(uint64_t *tt, uint64_t L, int N, int lv) {
     const uint64_t data = N - 1 >= 16 ? ~0ull : ((1ull << (4 * (N - 1))) - 1ull);
     const uint64_t key = L & data & 0x0fffffffffffffffull;
