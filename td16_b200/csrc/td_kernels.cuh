@@ -716,6 +716,10 @@ __device__ __forceinline__ int td_donate(td_warp_smem &s, const td_donate_ctx &d
 // instance.
 
 #define TD_TT_EMPTY 0xffffffffffffffffull  // no state has fifteen nibbles of 15
+// A unit starts using its table after this many expansions: most searches of
+// uniform permutations end sooner, and then clearing the table would cost
+// more than it saves.  States expanded before are simply not recorded.
+#define TD_TT_AFTER 32
 #define TD_TT_LOW60 0x0fffffffffffffffull
 
 __device__ __forceinline__ void td_tt_clear(const td_search_limits &lim) {
@@ -780,15 +784,12 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
         if (found >= 0) found = td_tri_table[tri_base + T - 1 - found];
     } else {
         td_unpack_state(s, d0, s.L[d0], s.off[d0], N);
-        if (lim.tt) {
-            td_tt_clear(lim);
-            (void)td_tt_visit(s, lim, d0, N);
-        }
         const int odd = td_prepare_rows(s, d0, N, O, F);
         found = td_evaluate_rows(s, code, N, d0, odd, O, F);
     }
     r.expansions = 1;
     int since_check = 0;
+    bool tt_on = false;  // the table is in use (free order, after TD_TT_AFTER expansions)
     for (;;) {
         if (found >= 0) {
             r.found_move = (uint16_t)found;
@@ -874,7 +875,13 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
         } else {
             if (lane == 0) s.path[level] = (uint16_t)t;
             td_apply_bytes(s, level, t, N);
-            if (lim.tt && td_tt_visit(s, lim, level + 1, N)) continue;  // explored with at least this budget
+            if (lim.tt) {
+                if (!tt_on && r.expansions >= TD_TT_AFTER) {
+                    td_tt_clear(lim);
+                    tt_on = true;
+                }
+                if (tt_on && td_tt_visit(s, lim, level + 1, N)) continue;  // explored with at least this budget
+            }
             ++level;
             const int odd = td_prepare_rows(s, level, N, O, F);
             found = td_evaluate_rows(s, code, N, level, odd, O, F);

@@ -260,8 +260,7 @@ bool tt_visit(uint64_t *tt, uint64_t L, int N, int lv) {
 
 int search_rows(Emu &e, td_result *res) {
     static thread_local uint64_t tt[1 << EMU_TT_BITS];
-    for (int q = 0; q < (1 << EMU_TT_BITS); ++q) tt[q] = ~0ull;
-    tt_visit(tt, e.L[0], e.N, 0);
+    bool tt_on = false;  // in use after 32 expansions, as in the kernel
     const int NP = (e.N - 1) * (e.N - 2) / 2;
     e.rounds = (NP + 31) / 32;
     for (int r = 0; r < TD_MAX_ROUNDS; ++r)
@@ -287,7 +286,11 @@ int search_rows(Emu &e, td_result *res) {
         int noff;
         td_apply_move(e.L[level], e.off[level], e.N, t & 31, (t >> 5) & 31, (t >> 10) & 31, &e.L[level + 1], &noff);
         e.off[level + 1] = noff;
-        if (tt_visit(tt, e.L[level + 1], e.N, level + 1)) continue;  // explored with at least this budget
+        if (!tt_on && e.expansions >= 32) {
+            for (int q = 0; q < (1 << EMU_TT_BITS); ++q) tt[q] = ~0ull;
+            tt_on = true;
+        }
+        if (tt_on && tt_visit(tt, e.L[level + 1], e.N, level + 1)) continue;  // explored with at least this budget
         ++level;
         odd = prepare_rows(e, e.L[level], e.off[level]);
         found = evaluate_rows(e, level, odd);
