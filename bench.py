@@ -41,13 +41,14 @@ WORKLOAD = "full-size decision search: 2^20 S_16 perms, 50% uniform / 50% revers
 # Per node expansion at N = 17, the search kernel's warp instructions (all
 # pipes) and those of the integer ALU pipe, and its DRAM bytes per launch:
 # ncu capture of td_steal_kernel on 65,536 copies of one S_16 instance (tuned
-# launch shape), summarised in profiles/td_steal_kernel_s16_replicated_64k.md:
-# 36.611 G warp instructions over 61.897 M expansions; the ALU pipe busy
-# 84.886% of 2 warp instructions per cycle over 13.539 G SM cycles; 2.24 MB of
-# DRAM traffic.
-INST_PER_EXPANSION = 36.611e9 / 61.897e6
-ALU_INST_PER_EXPANSION = 0.84886 * 2 * 13.539e9 / 61.897e6
-DRAM_BYTES_PER_64K_LAUNCH = 2.24e6
+# launch shape, explored-state tables on), summarised in
+# profiles/td_steal_kernel_s16_replicated_64k.md: 34.300 G warp instructions
+# over 44.254 M expansions (the instructions of children skipped through the
+# tables included); the ALU pipe busy 78.010% of 2 warp instructions per cycle
+# over 11.623 G SM cycles; 4.62 GB of DRAM traffic, mostly the tables.
+INST_PER_EXPANSION = 34.300e9 / 44.254e6
+ALU_INST_PER_EXPANSION = 0.78010 * 2 * 11.623e9 / 44.254e6
+DRAM_BYTES_PER_64K_LAUNCH = 4.62e9
 
 def rank_info():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
@@ -297,7 +298,8 @@ def run_engine(args):
                 "issue_peak_lop3_imad": issue_peak.value / 1e9,
                 "inst_per_expansion": INST_PER_EXPANSION,
                 "traffic": DRAM_BYTES_PER_64K_LAUNCH * count / 65536,
-                "traffic_note": "DRAM bytes per launch, ncu on 65,536 instances scaled by instance count",
+                "traffic_note": "DRAM bytes per launch, ncu on 65,536 replicated instances scaled by instance count "
+                                "(mostly the explored-state tables, which only long searches use)",
                 "nodes_per_s": nodes_per_s, "triples_per_s": triples_per_s}
 
     graph.close()
