@@ -833,30 +833,49 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
                 break;
             }
         }
-        uint32_t t;
-        if constexpr (ORDERED) {
-            int accepted;
-            const int u = td_next_child<true>(s, level, &accepted);
-            if (u < 0) {
-                if (level == d0) break;  // this subtree is exhausted
-                --level;
-                continue;
-            }
-            t = td_tri_table[tri_base + T - 1 - u];
-            if (accepted) {
-                r.found_move = (uint16_t)t;
-                r.depth = level + 1;
-                r.status = TD_DFS_FOUND;
+        // walk to the next node to expand: backtracks, and in free order the
+        // children skipped through the table, change no expansion count, so
+        // the checks above run once per expansion
+        uint32_t t = 0;
+        int walk = 0;  // 1: the subtree is exhausted, 2: a root accepted on visit (ordered)
+        for (;;) {
+            if constexpr (ORDERED) {
+                int accepted;
+                const int u = td_next_child<true>(s, level, &accepted);
+                if (u < 0) {
+                    if (level == d0) { walk = 1; break; }
+                    --level;
+                    continue;
+                }
+                t = td_tri_table[tri_base + T - 1 - u];
+                if (accepted) walk = 2;
+                break;
+            } else {
+                const int m = td_next_child_rows(s, code, level);
+                if (m < 0) {
+                    if (level == d0) { walk = 1; break; }
+                    --level;
+                    continue;
+                }
+                t = (uint32_t)m;
+                if (lane == 0) s.path[level] = (uint16_t)t;
+                td_apply_bytes(s, level, t, N);
+                if (lim.tt) {
+                    if (!tt_on && r.expansions >= TD_TT_AFTER) {
+                        td_tt_clear(lim);
+                        tt_on = true;
+                    }
+                    if (tt_on && td_tt_visit(s, lim, level + 1, N)) continue;  // explored with at least this budget
+                }
                 break;
             }
-        } else {
-            const int m = td_next_child_rows(s, code, level);
-            if (m < 0) {
-                if (level == d0) break;  // this subtree is exhausted
-                --level;
-                continue;
-            }
-            t = (uint32_t)m;
+        }
+        if (walk == 1) break;
+        if (walk == 2) {
+            r.found_move = (uint16_t)t;
+            r.depth = level + 1;
+            r.status = TD_DFS_FOUND;
+            break;
         }
         if constexpr (ORDERED) {
             uint64_t nL;
@@ -873,15 +892,6 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
             found = td_evaluate<true>(s, lut, code, steps, level, odd, maxd);
             if (found >= 0) found = td_tri_table[tri_base + T - 1 - found];
         } else {
-            if (lane == 0) s.path[level] = (uint16_t)t;
-            td_apply_bytes(s, level, t, N);
-            if (lim.tt) {
-                if (!tt_on && r.expansions >= TD_TT_AFTER) {
-                    td_tt_clear(lim);
-                    tt_on = true;
-                }
-                if (tt_on && td_tt_visit(s, lim, level + 1, N)) continue;  // explored with at least this budget
-            }
             ++level;
             const int odd = td_prepare_rows(s, level, N, O, F);
             found = td_evaluate_rows(s, code, N, level, odd, O, F);
