@@ -107,3 +107,22 @@ def test_search_stats_windows():
     c = s2.snapshot(2100)
     assert (a.busy_nanos, b.busy_nanos, c.busy_nanos, c.completed, c.started) == (400, 300, 200, 1, 0)
     assert c.latency_p50_ms == pytest.approx((2000 - 1000) / 1e6)
+
+
+def test_configuration_arguments_are_checked(td):
+    """The tuning entry points reject out-of-range values (no GPU needed) and
+    leave the configuration unchanged when they do."""
+    lib = td._lib.lib()
+    INVALID = td._lib.INVALID_ARG
+    for bits in (-1, 1, 5, 17, 40):
+        assert lib.td_configure_table(bits) == INVALID
+    for args in ((0, 2, 32), (1, -1, 32), (1, 9, 32), (1, 2, 0)):
+        assert lib.td_configure_serve(*args) == INVALID
+        assert lib.td_configure_steal(*args) == INVALID
+    # valid values (the defaults) are accepted
+    assert lib.td_configure_table(12) == td._lib.OK
+    assert lib.td_configure_table(0) == td._lib.OK
+    assert lib.td_configure_table(12) == td._lib.OK
+    assert lib.td_configure_serve(1, 2, 32) == td._lib.OK
+    with pytest.raises(td.TdError):
+        td._lib.configure_table(3)

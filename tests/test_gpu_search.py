@@ -227,3 +227,28 @@ def test_cuda_graph_replays_match_eager_launches(slots):
             assert (res["status"] == eager["status"]).all()  # -6 would mark a witness failing replay
     finally:
         g.close()
+
+
+def test_explored_state_tables_keep_verdicts(slots, oracle):
+    """Free order with and without the per-warp tables of explored states, on
+    hard n = 12..13 instances at their bound (several end without a witness):
+    identical verdicts, equal to the oracle's on a sample, and every witness
+    replays; the tables cut expansions."""
+    td = slots
+    perms, n = td.synth_perms(8, 4096, 12, 13, 100, 1, 3)
+    maxd = (n // 2 + 1).astype(np.int32)
+    inst = td.prepare_perms(perms, n, maxd)
+    try:
+        td._lib.configure_table(0)
+        plain, st0 = td.search_batch(0, inst, 0)
+        td._lib.configure_table(12)
+        tabled, st1 = td.search_batch(0, inst, 0)
+    finally:
+        td._lib.configure_table(12)
+    assert (plain["status"] == tabled["status"]).all() and st0.errors == st1.errors == 0
+    assert st1.expansions < st0.expansions
+    beta, omega, init, N = _pairs(oracle, perms[:200], n[:200])
+    ost, _, _, _ = _oracle_batch(oracle, beta, omega, N, init, 0.0, maxd[:200], 1)
+    assert (tabled["status"][:200] == ost).all()
+    b2, o2, _, N2 = _pairs(oracle, perms, n)
+    _replay_all(oracle, b2, o2, N2, tabled, maxd)
