@@ -203,10 +203,18 @@ def synth_perms(seed: int, count: int, n_min: int, n_max: int, hard_pct: int, ha
     return perms, n
 
 
-def search_batch(slot: int, instances: np.ndarray, flags: int = 0, max_expansions: int = 0):
-    """Host arrays in and out.  Returns (results, BatchStats)."""
+def search_batch(slot: int, instances: np.ndarray, flags: int = 0, max_expansions: int = 0, out=None):
+    """Host arrays in and out.  Returns (results, BatchStats).  `out`, when
+    given, is a contiguous RESULT_DTYPE array of the same length that receives
+    the results (e.g. a view of pinned host memory, so that the copies run at
+    full PCIe speed)."""
     instances = np.ascontiguousarray(instances, INSTANCE_DTYPE)
-    results = np.zeros(len(instances), RESULT_DTYPE)
+    if out is None:
+        results = np.zeros(len(instances), RESULT_DTYPE)
+    else:
+        results = out
+        if results.dtype != RESULT_DTYPE or len(results) != len(instances) or not results.flags["C_CONTIGUOUS"]:
+            raise TdError(INVALID_ARG, "out must be a contiguous result array of the batch's length")
     st = BatchStats()
     err = C.create_string_buffer(512)
     rc = lib().td_search_batch(int(slot), len(instances), _ptr(instances), _ptr(results), int(flags),
