@@ -40,15 +40,15 @@ UNIT = "witnesses/s"
 WORKLOAD = "full-size decision search: 2^20 S_16 perms, 50% uniform / 50% reverse o 1-4 transpositions, d<=9"
 # Per node expansion at N = 17, the search kernel's warp instructions (all
 # pipes) and those of the integer ALU pipe, and its DRAM bytes per launch:
-# ncu capture of td_steal_kernel on 65,536 copies of one S_16 instance (tuned
-# launch shape, explored-state tables on), summarised in
-# profiles/td_steal_kernel_s16_replicated_64k.md: 34.300 G warp instructions
-# over 44.254 M expansions (the instructions of children skipped through the
-# tables included); the ALU pipe busy 78.010% of 2 warp instructions per cycle
-# over 11.623 G SM cycles; 4.62 GB of DRAM traffic, mostly the tables.
-INST_PER_EXPANSION = 34.300e9 / 44.254e6
-ALU_INST_PER_EXPANSION = 0.78010 * 2 * 11.623e9 / 44.254e6
-DRAM_BYTES_PER_64K_LAUNCH = 4.62e9
+# ncu capture of td_steal_kernel on the first 2^18 instances of this workload
+# (tuned launch shape, explored-state tables on), summarised in
+# profiles/td_steal_kernel_s16_mix_2p18.md: 48.197 G warp instructions over
+# 55.299 M expansions (skipped children, donation and scheduling included);
+# the ALU pipe busy 71.312% of 2 warp instructions per cycle over 17.614 G SM
+# cycles; 5.43 GB of DRAM traffic, mostly the explored-state tables.
+INST_PER_EXPANSION = 48.197e9 / 55.299e6
+ALU_INST_PER_EXPANSION = 0.71312 * 2 * 17.614e9 / 55.299e6
+DRAM_BYTES_PER_2P18_LAUNCH = 5.43e9
 
 def rank_info():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
@@ -302,9 +302,9 @@ def run_engine(args):
                 "issue_achieved": nodes_per_s * INST_PER_EXPANSION / 1e9,
                 "issue_peak_lop3_imad": issue_peak.value / 1e9,
                 "inst_per_expansion": INST_PER_EXPANSION,
-                "traffic": DRAM_BYTES_PER_64K_LAUNCH * count / 65536,
-                "traffic_note": "DRAM bytes per launch, ncu on 65,536 replicated instances scaled by instance count "
-                                "(mostly the explored-state tables, which only long searches use)",
+                "traffic": DRAM_BYTES_PER_2P18_LAUNCH * count / (1 << 18),
+                "traffic_note": "DRAM bytes per launch: ncu on the first 2^18 instances, scaled by instance count "
+                                "(mostly the explored-state tables)",
                 "nodes_per_s": nodes_per_s, "triples_per_s": triples_per_s}
 
     graph.close()
