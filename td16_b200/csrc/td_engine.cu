@@ -58,10 +58,14 @@ static_assert(sizeof(td_result) == 32, "td_result layout");
 // Class table (td_class_of_index for every 12-bit index), filled by the host.
 __device__ __align__(16) uint8_t td_lut_global[TD_LUT_BYTES];
 
+// Copies the class table into shared memory (kernels of the reference order;
+// `lut` is null in the free-order batch kernel, which does not use it).
 __device__ __forceinline__ void td_block_init(uint8_t *lut, td_warp_smem *ws, int warps) {
-    const uint4 *src = reinterpret_cast<const uint4 *>(td_lut_global);
-    uint4 *dst = reinterpret_cast<uint4 *>(lut);
-    for (int i = threadIdx.x; i < TD_LUT_BYTES / 16; i += blockDim.x) dst[i] = src[i];
+    if (lut) {
+        const uint4 *src = reinterpret_cast<const uint4 *>(td_lut_global);
+        uint4 *dst = reinterpret_cast<uint4 *>(lut);
+        for (int i = threadIdx.x; i < TD_LUT_BYTES / 16; i += blockDim.x) dst[i] = src[i];
+    }
     for (int w = 0; w < warps; ++w)
         for (int b = threadIdx.x; b < TD_PT_STRIDE; b += blockDim.x) ws[w].pt[TD_PT_DUMMY + b] = 0;
     __syncthreads();
@@ -167,7 +171,10 @@ __device__ __forceinline__ int td_finish_unit(const td_dfs_out &r, td_inst_state
     return last;
 }
 
-__global__ void __launch_bounds__(256, 4) td_steal_kernel(const td_instance *__restrict__ in,
+#ifndef TD_STEAL_MIN_BLOCKS
+#define TD_STEAL_MIN_BLOCKS 4  // resident blocks of 8 warps per SM the register budget is sized for
+#endif
+__global__ void __launch_bounds__(256, TD_STEAL_MIN_BLOCKS) td_steal_kernel(const td_instance *__restrict__ in,
                                                       td_result *__restrict__ out, int count, td_pool *pool,
                                                       td_item *items, uint32_t *ready, const uint32_t *epoch_ptr,
                                                       int capacity, td_inst_state *state, int grain,
@@ -175,9 +182,10 @@ __global__ void __launch_bounds__(256, 4) td_steal_kernel(const td_instance *__r
                                                       uint64_t *tt, int tt_bits) {
     extern __shared__ __align__(16) uint8_t td_smem[];
     const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint8_t *lut = td_smem;
-    td_warp_smem *ws = reinterpret_cast<td_warp_smem *>(td_smem + TD_LUT_BYTES);
-    td_block_init(lut, ws, warps);
+    // free order only: no class table, the warp frames start the block's shared memory
+    const uint8_t *lut = nullptr;
+    td_warp_smem *ws = reinterpret_cast<td_warp_smem *>(td_smem);
+    td_block_init(nullptr, ws, warps);
     td_warp_smem &s = ws[warp];
     uint32_t code[TD_MAX_STEPS];
     int codeN = -1;
@@ -459,6 +467,8 @@ std::string cuda_msg(cudaError_t e, const char *file, int line) {
     } while (0)
 
 size_t smem_bytes(int warps) { return TD_LUT_BYTES + (size_t)warps * sizeof(td_warp_smem); }
+// td_steal_kernel keeps no class table
+size_t steal_smem_bytes(int warps) { return (size_t)warps * sizeof(td_warp_smem); }
 
 std::atomic<uint64_t> g_time_limit_ns{0};
 
@@ -565,7 +575,7 @@ int launch_batch(Slot &s, int count, const td_instance *d_in, td_result *d_out, 
         DeviceInfo &d = g_dev[s.device];
         if (d.steal_blocks_per_sm == 0) {
             int b = 0;
-            TD_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, td_steal_kernel, threads, smem));
+            TD_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, td_steal_kernel, threads, steal_smem_bytes(warps)));
             d.steal_blocks_per_sm = std::max(1, b);
         }
         // at least the slot's share of the resident grid, so that a small batch
@@ -588,7 +598,8 @@ int launch_batch(Slot &s, int count, const td_instance *d_in, td_result *d_out, 
         TD_CHECK(cudaMemsetAsync(s.d_pool, 0, sizeof(td_pool), stream));
         TD_CHECK(cudaMemsetAsync(s.d_state, 0, (size_t)count * sizeof(td_inst_state), stream));
         td_epoch_kernel<<<1, 1, 0, stream>>>(s.d_epoch);
-        td_steal_kernel<<<grid, threads, smem, stream>>>(d_in, d_out, count, s.d_pool, s.d_items, s.d_ready, s.d_epoch,
+        td_steal_kernel<<<grid, threads, steal_smem_bytes(warps), stream>>>(d_in, d_out, count, s.d_pool, s.d_items,
+                                                                            s.d_ready, s.d_epoch,
                                                          s.item_capacity, s.d_state, g_steal_grain, g_split_level,
                                                          g_check_every, time_limit_ns(), g_tt_bits > 0 ? s.d_tt : nullptr,
                                                          g_tt_bits);
