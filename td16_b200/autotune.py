@@ -29,8 +29,8 @@ DEFAULT = {"warps": 4, "grain": 4, "split_level": 4, "check_every": 8}
 GRID = {
     "warps": [4, 8],
     "grain": [1, 2, 4],
-    "split_level": [2, 3, 4],
-    "check_every": [64, 256, 512, 1024],
+    "split_level": [2, 3, 4, 6],
+    "check_every": [64, 128, 256, 512, 1024],
 }
 QUICK = {"warps": [2, 4], "grain": [4, 8], "split_level": [4], "check_every": [32, 128]}
 
@@ -67,11 +67,11 @@ def tune_bucket(slot: int, instances: np.ndarray, grid=None, repeats: int = 2, l
 
 
 def buckets(quick: bool):
-    """Sample workloads per bucket: the batched mix (n 11..13) and S_16 (2^18
-    instances, so that the launch tail weighs about as much as in a full-size
-    batch)."""
+    """Sample workloads per bucket: the batched mix (n 11..13; 65,536 instances,
+    the batch it is run as) and S_16 (2^18 instances, so that the launch tail
+    weighs about as much as in a full-size batch)."""
     c = 4096 if quick else 16384
-    mix = _lib.synth_perms(1, c, 11, 13, 25, 1, 3)
+    mix = _lib.synth_perms(1, c if quick else 65536, 11, 13, 25, 1, 3)
     s16 = _lib.synth_perms(2, c if quick else 1 << 18, 16, 16, 50, 1, 4)
     return {
         "mix_11_13": _lib.prepare_perms(mix[0], mix[1], (mix[1] // 2 + 1).astype(np.int32)),
