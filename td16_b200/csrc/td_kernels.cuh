@@ -1,15 +1,24 @@
 // td_kernels.cuh -- the sm_100a witness-search warp engine.
 //
-// One warp owns one search (a DFS over move sequences).  Per node it
-//   1. labels the omega cycles of the pinned state with warp pointer jumping
-//      (lane p = pinned position p; leader = smallest position, dist = steps
-//      to the leader, len = cycle length; 5 rounds cover cycles up to 32),
-//   2. writes the pair table (4 bits per ordered pair of caller positions),
-//   3. evaluates every triple: lane l takes u = 32*s + l in step s, reads three
-//      pair entries and one class-table byte (no pointer chasing), and keeps
-//      one bit per step in per-lane masks (found / first-choice / second-choice),
-//   4. picks the next child with a warp max-reduction over the masks in the
-//      reference's single-queue order (ordered mode) or +2 moves first.
+// One warp owns one search (a DFS over move sequences), or one donated
+// subtree of it.  Two node evaluations share the DFS:
+//
+// Reference order (td_prepare_node, td_evaluate, td_next_child): per node the
+// warp labels the omega cycles of the pinned state by pointer jumping (lane p
+// = pinned position p), writes the pair table (4 bits per ordered pair of
+// caller positions), and evaluates every triple: lane l takes u = 32*s + l in
+// step s, reads three pair entries and one class-table byte, and keeps one bit
+// per step in per-lane masks.  The next child comes from a warp max-reduction
+// in the reference's single-queue order.
+//
+// Free order (td_prepare_rows, td_evaluate_rows, td_next_child_rows): the
+// state is the caller's array, one byte per position; per node the warp builds
+// cycle row masks (one per caller position), and each lane classifies all the
+// children (i, j, k) of its pair slots at once with LOP3 logic
+// (td_row_classes).  The next child, +2 moves first, comes from per-level lane
+// summaries.  A table of explored states skips children reached before by
+// another move order, and busy warps donate subtrees to idle ones.
+//
 // Reference: emitter/src/native/backtracking/sorting_search.cu:478-712.
 #pragma once
 
