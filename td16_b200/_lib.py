@@ -52,7 +52,7 @@ _lib = None
 EXPORTS = ["td_init_slots", "td_search", "td_search_ordered", "td_slot_count", "td_slot_device",
            "td_slot_stream", "td_destroy", "td_prepare_pairs", "td_prepare_perms", "td_synth_perms",
            "td_search_batch", "td_search_batch_device", "td_validate_batch_device",
-           "td_positions_to_symbols", "td_configure", "td_configure_steal", "td_configure_serve", "td_configure_table",
+           "td_positions_to_symbols", "td_configure", "td_configure_steal", "td_configure_serve", "td_configure_table", "td_configure_restart",
            "td_set_time_limit", "td_int_issue_peak",
            "td_codec_key", "td_codec_value", "td_codec_decode_key", "td_codec_decode_value",
            "td_replay_symbols_device", "td_cert_writer_open", "td_cert_writer_enqueue", "td_cert_writer_close",
@@ -91,6 +91,7 @@ def lib():
     L.td_configure_steal.argtypes = [C.c_int, C.c_int, C.c_int]
     L.td_configure_serve.argtypes = [C.c_int, C.c_int, C.c_int]
     L.td_configure_table.argtypes = [C.c_int]
+    L.td_configure_restart.argtypes = [C.c_int]
     L.td_set_time_limit.argtypes = [C.c_double]
     L.td_codec_key.argtypes = [vp, C.c_int, vp, C.c_int]
     L.td_codec_value.argtypes = [vp, C.c_int, vp, C.c_int]
@@ -267,6 +268,12 @@ def configure_table(bits: int) -> None:
     """Explored-state tables of the free order: 2^bits entries per warp, 0 = none."""
     if lib().td_configure_table(int(bits)) != OK:
         raise TdError(INVALID_ARG, "table bits must be 0 or 6..16")
+
+
+def configure_restart(base: int) -> None:
+    """Restart budgets of free-order batch searches: base x Luby sequence, 0 = none."""
+    if lib().td_configure_restart(int(base)) != OK:
+        raise TdError(INVALID_ARG, "restart base must be 0 or >= 16")
 
 
 def configure_serve(grain: int, split_level: int, check_every: int) -> None:

@@ -6,6 +6,8 @@ launch on a sample for every point of a grid over
   steal granularity (items per donation),
   split depth (deepest DFS level whose children may be donated),
   check interval (expansions between idle checks),
+and then, with the winning shape, the restart budget base of the root searches
+(0 = no restarts),
 keeps the fastest by device time, and stores the winners per bucket in
 td16_b200/tuned.json.  `apply(N)` configures the engine for a bucket.
 
@@ -24,7 +26,7 @@ import numpy as np
 from . import _lib
 
 TUNED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned.json")
-DEFAULT = {"warps": 4, "grain": 4, "split_level": 4, "check_every": 8}
+DEFAULT = {"warps": 4, "grain": 4, "split_level": 4, "check_every": 8, "restart": 0}
 
 GRID = {
     "warps": [4, 8],
@@ -35,9 +37,13 @@ GRID = {
 QUICK = {"warps": [2, 4], "grain": [4, 8], "split_level": [4], "check_every": [32, 128]}
 
 
+RESTARTS = [0, 32, 64, 128, 256]
+
+
 def _configure(p):
     _lib.configure(p["warps"], 1)
     _lib.configure_steal(p["grain"], p["split_level"], p["check_every"])
+    _lib.configure_restart(p.get("restart", 0))
 
 
 def time_point(slot: int, instances: np.ndarray, params: dict, repeats: int = 2) -> float:
@@ -62,6 +68,14 @@ def tune_bucket(slot: int, instances: np.ndarray, grid=None, repeats: int = 2, l
         log(f"  {p} -> {ms:.2f} ms")
     results.sort(key=lambda r: r[0])
     best_ms, best = results[0]
+    # then the restart budget base with the winning launch shape
+    for base in RESTARTS:
+        p = dict(best, restart=base)
+        ms = time_point(slot, instances, p, repeats)
+        results.append((ms, p))
+        log(f"  {p} -> {ms:.2f} ms")
+        if ms < best_ms:
+            best_ms, best = ms, p
     _configure(DEFAULT)
     return {"params": best, "kernel_ms": best_ms, "points": len(results)}
 

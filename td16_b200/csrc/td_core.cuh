@@ -241,6 +241,44 @@ TD_HD uint32_t td_pair_code(int N, int q) {
     return (uint32_t)i | ((uint32_t)j << 5) | ((uint32_t)j << 10) | ((uint32_t)(31 - j) << 15);
 }
 
+// ---- restarts of the free order ----------------------------------------------
+//
+// The free-order search has a heavy tail: on near-reverse S_16 the median
+// search takes ~30 expansions and a few take tens of thousands, because an
+// early wrong turn leads into a large subtree without a witness.  A search
+// therefore restarts with another child order after a budget of expansions;
+// the budgets follow the Luby sequence (base x 1, 1, 2, 1, 1, 2, 4, ...), and
+// the attempt after TD_RESTARTS ends is unbounded, so a search without a
+// witness still completes.  Restarting never changes a verdict: every attempt
+// explores a subtree order of the same tree, and the last one all of it.
+
+#define TD_RESTARTS 24  // attempts with a budget; the next one runs to the end
+
+// The i-th term (i >= 1) of the Luby sequence 1, 1, 2, 1, 1, 2, 4, 1, 1, ...
+TD_HD uint32_t td_luby(uint32_t i) {
+    for (;;) {
+        uint32_t k = 1;
+        while (((1u << k) - 1u) < i) ++k;
+        if (i == (1u << k) - 1u) return 1u << (k - 1);
+        i -= (1u << (k - 1)) - 1u;
+    }
+}
+
+// Expansion budget of attempt a (0-based) for a base budget; ~0u = unbounded.
+TD_HD uint32_t td_attempt_budget(uint32_t base, int a) {
+    if (base == 0 || a >= TD_RESTARTS) return ~0u;
+    const uint64_t b = (uint64_t)base * td_luby((uint32_t)a + 1u);
+    return b >= 0xffffffffull ? ~0u : (uint32_t)b;
+}
+
+// Child order of attempt a: bits 0-4 rotate the lane priority, bit 5 takes
+// the lowest pair round of a lane first, bit 6 the largest k first.  Attempt 0
+// is the plain free order.
+TD_HD uint32_t td_order_variant(int a) {
+    if (a == 0) return 0u;
+    return ((uint32_t)(7 * a) & 31u) | (((uint32_t)a & 1u) << 5) | ((((uint32_t)a >> 1) & 1u) << 6);
+}
+
 // Per-position cycle descriptor: leader (smallest pinned position of the
 // cycle), dist (omega steps to the leader), len (cycle length).
 TD_HD uint32_t td_pair_entry(int leader_p, int dist_p, int len_p, int leader_q,

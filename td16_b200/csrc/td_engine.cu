@@ -54,6 +54,7 @@ static_assert(sizeof(td_result) == 32, "td_result layout");
 
 #define TD_LUT_BYTES 4096
 #define TD_TT_BITS 12  // default: 4096 explored-state entries (32 KiB) per warp of a free-order launch
+#define TD_RESTART_BASE 200  // default base of the free order's restart budgets (expansions)
 
 // Class table (td_class_of_index for every 12-bit index), filled by the host.
 __device__ __align__(16) uint8_t td_lut_global[TD_LUT_BYTES];
@@ -79,6 +80,7 @@ __device__ __forceinline__ td_search_limits td_make_limits(uint64_t max_exp, uin
     lim.abort_flag = abort_flag;
     lim.tt = nullptr;
     lim.tt_bits = 0;
+    lim.restart_base = 0;
     return lim;
 }
 
@@ -179,7 +181,7 @@ __global__ void __launch_bounds__(256, TD_STEAL_MIN_BLOCKS) td_steal_kernel(cons
                                                       td_item *items, uint32_t *ready, const uint32_t *epoch_ptr,
                                                       int capacity, td_inst_state *state, int grain,
                                                       int max_level, int check_every, uint64_t time_limit_ns,
-                                                      uint64_t *tt, int tt_bits) {
+                                                      uint64_t *tt, int tt_bits, uint32_t restart_base) {
     extern __shared__ __align__(16) uint8_t td_smem[];
     const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // free order only: no class table, the warp frames start the block's shared memory
@@ -190,6 +192,7 @@ __global__ void __launch_bounds__(256, TD_STEAL_MIN_BLOCKS) td_steal_kernel(cons
     uint32_t code[TD_MAX_STEPS];
     int codeN = -1;
     td_search_limits lim = td_make_limits(0, time_limit_ns, nullptr);
+    lim.restart_base = restart_base;
     if (tt) {
         lim.tt = tt + ((size_t)(blockIdx.x * warps + warp) << tt_bits);
         lim.tt_bits = tt_bits;
@@ -311,9 +314,13 @@ __global__ void __launch_bounds__(256, TD_STEAL_MIN_BLOCKS) td_steal_kernel(cons
                     r.found_move = 0;
                     r.expansions = 0;
                 } else {
+                    // a donated subtree is searched once, to the end: restarting it
+                    // would only repeat work when it holds no witness
+                    td_search_limits ilim = lim;
+                    ilim.restart_base = 0;
                     dc.inst = idx;
                     dc.state = st;
-                    r = td_dfs<false>(s, lut, code, x.n_symbols, x.max_moves, d0, lim, &dc);
+                    r = td_dfs<false>(s, lut, code, x.n_symbols, x.max_moves, d0, ilim, &dc);
                 }
                 td_finish_unit(r, st, &out[idx], s.path);
             }
@@ -445,6 +452,7 @@ int g_serve_grain = 1;
 int g_serve_split_level = 2;
 int g_serve_check_every = 32;
 int g_tt_bits = TD_TT_BITS;  // log2 entries of the explored-state tables; 0 = no table
+uint32_t g_restart_base = TD_RESTART_BASE;  // free-order restart budget base; 0 = no restarts
 
 void set_err(char *err, size_t len, const std::string &msg) {
     if (err && len) {
@@ -602,7 +610,7 @@ int launch_batch(Slot &s, int count, const td_instance *d_in, td_result *d_out, 
                                                                             s.d_ready, s.d_epoch,
                                                          s.item_capacity, s.d_state, g_steal_grain, g_split_level,
                                                          g_check_every, time_limit_ns(), g_tt_bits > 0 ? s.d_tt : nullptr,
-                                                         g_tt_bits);
+                                                         g_tt_bits, g_restart_base);
     } else {
         DeviceInfo &d = g_dev[s.device];
         if (d.blocks_per_sm == 0) {
@@ -895,6 +903,17 @@ TD_API int td_configure_table(int bits) {
     if (bits != 0 && (bits < 6 || bits > 16)) return TD_INVALID_ARG;
     std::lock_guard<std::mutex> g(g_mu);
     g_tt_bits = bits;
+    return TD_OK;
+}
+
+// Restarts of later free-order batch searches: a search that has spent
+// base x luby(a) expansions in attempt a starts again with another child order
+// (td_attempt_budget, td_order_variant); 0 turns restarts off.  Verdicts do
+// not depend on it.
+TD_API int td_configure_restart(int base) {
+    if (base < 0 || (base > 0 && base < 16)) return TD_INVALID_ARG;
+    std::lock_guard<std::mutex> g(g_mu);
+    g_restart_base = (uint32_t)base;
     return TD_OK;
 }
 
@@ -1295,7 +1314,7 @@ TD_API int td_search_batch_noalloc(int count, const td_instance *d_instances, td
         const int grid = std::max(1, std::min(d.sms * std::max(1, d.steal_blocks), blocks_needed));
         td_steal_kernel<<<grid, threads, smem, st>>>(d_instances, d_results, count, pool, items, ready, epoch,
                                                      TD_NOALLOC_ITEMS, state, g_steal_grain, g_split_level,
-                                                     g_check_every, limit, nullptr, 0);
+                                                     g_check_every, limit, nullptr, 0, g_restart_base);
     }
     TD_CHECK_NA(cudaGetLastError());
     if (flags & TD_FLAG_VERIFY) {

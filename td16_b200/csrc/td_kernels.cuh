@@ -216,6 +216,7 @@ struct td_search_limits {
     const int *abort_flag;     // optional host/device abort request
     uint64_t *tt;              // this warp's table of explored states (free order); null = none
     int tt_bits;               // log2 of its entries
+    uint32_t restart_base;     // free order: base of the restart budgets (td_attempt_budget); 0 = none
 };
 
 __device__ __forceinline__ uint64_t td_globaltimer() {
@@ -494,26 +495,37 @@ __device__ __forceinline__ int td_evaluate_rows(td_warp_smem &s, const uint32_t 
     return -1;
 }
 
-// Next child of `level` in the free order: +2 children first; among them the
-// highest pair slot (the lexicographically smallest pair) and its smallest k.
+// Next child of `level` in the free order: +2 children first; among them, in
+// the plain order (ord = 0), the highest pair slot (the lexicographically
+// smallest pair) and its smallest k.  `ord` (td_order_variant) rotates the
+// lane priority, reverses the round order and takes the largest k first.
 // Returns the move or -1.
 __device__ __forceinline__ int td_next_child_rows(td_warp_smem &s, const uint32_t (&code)[TD_MAX_STEPS],
-                                                  int level) {
+                                                  int level, uint32_t ord) {
     const int lane = threadIdx.x & 31;
     const uint32_t m2 = s.m2[level], m0 = s.m0[level];
     if ((m2 | m0) == 0) return -1;
     const bool c2 = m2 != 0;
     const uint32_t lanes = c2 ? m2 : m0;
-    const int win = 31 - __clz(lanes);
+    const uint32_t rot = ord & 31u;
+    // the lane with the largest (lane - rot) mod 32
+    const int win = (int)(((31u - (uint32_t)__clz(__funnelshift_r(lanes, lanes, rot))) + rot) & 31u);
     const uint4 Wv = s.pw[level][win];
     const uint32_t cm = c2 ? 0x0000ffffu : 0xffff0000u;
     int r;
     uint32_t w;
-    if (Wv.w & cm) { r = 3; w = Wv.w; }
-    else if (Wv.z & cm) { r = 2; w = Wv.z; }
-    else if (Wv.y & cm) { r = 1; w = Wv.y; }
-    else { r = 0; w = Wv.x; }
-    const int b = __ffs(w & cm) - 1;
+    if (ord & 32u) {
+        if (Wv.x & cm) { r = 0; w = Wv.x; }
+        else if (Wv.y & cm) { r = 1; w = Wv.y; }
+        else if (Wv.z & cm) { r = 2; w = Wv.z; }
+        else { r = 3; w = Wv.w; }
+    } else {
+        if (Wv.w & cm) { r = 3; w = Wv.w; }
+        else if (Wv.z & cm) { r = 2; w = Wv.z; }
+        else if (Wv.y & cm) { r = 1; w = Wv.y; }
+        else { r = 0; w = Wv.x; }
+    }
+    const int b = (ord & 64u) ? 31 - __clz(w & cm) : __ffs(w & cm) - 1;
     const uint32_t nw = w & ~(1u << b);
     const uint32_t mine = r == 3 ? code[3] : (r == 2 ? code[2] : (r == 1 ? code[1] : code[0]));
     const uint32_t pc = __shfl_sync(TD_FULL, mine, win);
@@ -799,6 +811,9 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
     r.expansions = 1;
     int since_check = 0;
     bool tt_on = false;  // the table is in use (free order, after TD_TT_AFTER expansions)
+    int attempt = 0;     // free order: restarts with another child order (td_attempt_budget)
+    uint32_t ord = 0, attempt_exp = 1;
+    uint32_t attempt_budget = ORDERED ? ~0u : td_attempt_budget(lim.restart_base, 0);
     for (;;) {
         if (found >= 0) {
             r.found_move = (uint16_t)found;
@@ -809,6 +824,23 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
         if (r.expansions >= lim.max_expansions) {
             r.status = TD_DFS_BUDGET;
             break;
+        }
+        if constexpr (!ORDERED) {
+            if (attempt_exp >= attempt_budget) {
+                // restart the subtree at d0 with the next child order; the table
+                // held nodes of the abandoned attempt that were not explored to
+                // the end, so it is cleared before its next use
+                ++attempt;
+                ord = td_order_variant(attempt);
+                attempt_budget = td_attempt_budget(lim.restart_base, attempt);
+                attempt_exp = 1;
+                tt_on = false;
+                level = d0;
+                const int odd = td_prepare_rows(s, d0, N, O, F);
+                found = td_evaluate_rows(s, code, N, d0, odd, O, F);
+                ++r.expansions;
+                continue;
+            }
         }
         if constexpr (!ORDERED) {
             if (dc && ++since_check >= dc->check_every) {
@@ -860,7 +892,7 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
                 if (accepted) walk = 2;
                 break;
             } else {
-                const int m = td_next_child_rows(s, code, level);
+                const int m = td_next_child_rows(s, code, level, ord);
                 if (m < 0) {
                     if (level == d0) { walk = 1; break; }
                     --level;
@@ -904,6 +936,7 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
             ++level;
             const int odd = td_prepare_rows(s, level, N, O, F);
             found = td_evaluate_rows(s, code, N, level, odd, O, F);
+            ++attempt_exp;
         }
         ++r.expansions;
     }

@@ -109,6 +109,7 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
     lim.abort_flag = nullptr;
     lim.tt = (!ORDERED && tt) ? tt + ((size_t)(blockIdx.x * warps + warp) << tt_bits) : nullptr;
     lim.tt_bits = tt_bits;
+    lim.restart_base = 0;  // serving searches are not restarted
     td_donate_ctx dc;
     dc.ring = 1;
     dc.deadline_ns = deadline;

@@ -147,22 +147,29 @@ int evaluate_rows(Emu &e, int level, int odd) {
     return best == 0xffffffffu ? -1 : (int)(best & 0x7fffu);
 }
 
-// Next child of `level` in the free order: +2 children first, the highest
-// pair slot R*lane + r (lexicographically smallest pair) and the smallest k.
-// Returns the move or -1.
-int next_child_rows(Emu &e, int level) {
+// Next child of `level` in the free order: +2 children first; in the plain
+// order (ord = 0) the highest pair slot R*lane + r (lexicographically smallest
+// pair) and the smallest k.  `ord` (td_order_variant) rotates the lane
+// priority, reverses the round order and takes the largest k first, as the
+// kernel does.  Returns the move or -1.
+int next_child_rows(Emu &e, int level, uint32_t ord) {
     bool any2 = false;
     for (int lane = 0; lane < 32; ++lane)
         for (int r = 0; r < e.rounds; ++r) any2 |= (e.pw[level][r][lane] & 0xffffu) != 0;
     const uint32_t cm = any2 ? 0x0000ffffu : 0xffff0000u;
-    int best = -1;
+    const int rot = (int)(ord & 31u);
+    int bl = -1, br = -1;
+    unsigned bkey = 0;
     for (int lane = 0; lane < 32; ++lane)
         for (int r = 0; r < e.rounds; ++r)
-            if (e.pw[level][r][lane] & cm) best = e.rounds * lane + r;
-    if (best < 0) return -1;
-    const int lane = best / e.rounds, r = best % e.rounds;
+            if (e.pw[level][r][lane] & cm) {
+                const unsigned key = ((((unsigned)(lane - rot) & 31u) << 2) | (unsigned)((ord & 32u) ? 3 - r : r)) + 1u;
+                if (key > bkey) { bkey = key; bl = lane; br = r; }
+            }
+    if (bl < 0) return -1;
+    const int lane = bl, r = br;
     const uint32_t w = e.pw[level][r][lane] & cm;
-    const int b = __builtin_ctz(w);
+    const int b = (ord & 64u) ? 31 - __builtin_clz(w) : __builtin_ctz(w);
     e.pw[level][r][lane] &= ~(1u << b);
     const int k = any2 ? b + 1 : b - 15;
     return (int)((e.pc[r][lane] & 1023u) | ((uint32_t)k << 10));
@@ -248,6 +255,9 @@ int next_child(Emu &e, int level, int *accepted) {
 // the low 15 nibbles of the pinned state (nibbles from N-1 on cleared), depth
 // in the top nibble, direct-mapped by a multiplicative hash.
 #define EMU_TT_BITS 12
+// restart budget base of the free order (the kernel's default); 0 = none
+static uint32_t g_restart_base = 200;
+extern "C" void td_emu_set_restart(uint32_t base) { g_restart_base = base; }
 bool tt_visit(uint64_t *tt, uint64_t L, int N, int lv) {
     const uint64_t data = N - 1 >= 16 ? ~0ull : ((1ull << (4 * (N - 1))) - 1ull);
     const uint64_t key = L & data & 0x0fffffffffffffffull;
@@ -261,6 +271,8 @@ bool tt_visit(uint64_t *tt, uint64_t L, int N, int lv) {
 int search_rows(Emu &e, td_result *res) {
     static thread_local uint64_t tt[1 << EMU_TT_BITS];
     bool tt_on = false;  // in use after 32 expansions, as in the kernel
+    int attempt = 0;     // restarts, as in the kernel
+    uint32_t ord = 0, attempt_exp = 1, attempt_budget = td_attempt_budget(g_restart_base, 0);
     const int NP = (e.N - 1) * (e.N - 2) / 2;
     e.rounds = (NP + 31) / 32;
     for (int r = 0; r < TD_MAX_ROUNDS; ++r)
@@ -276,7 +288,18 @@ int search_rows(Emu &e, td_result *res) {
             res->status = TD_FOUND;
             break;
         }
-        const int t = next_child_rows(e, level);
+        if (attempt_exp >= attempt_budget) {
+            ++attempt;
+            ord = td_order_variant(attempt);
+            attempt_budget = td_attempt_budget(g_restart_base, attempt);
+            attempt_exp = 1;
+            tt_on = false;
+            level = 0;
+            odd = prepare_rows(e, e.L[0], e.off[0]);
+            found = evaluate_rows(e, 0, odd);
+            continue;
+        }
+        const int t = next_child_rows(e, level, ord);
         if (t < 0) {
             if (level == 0) { res->status = TD_NOT_FOUND; break; }
             --level;
@@ -294,6 +317,7 @@ int search_rows(Emu &e, td_result *res) {
         ++level;
         odd = prepare_rows(e, e.L[level], e.off[level]);
         found = evaluate_rows(e, level, odd);
+        ++attempt_exp;
     }
     res->expansions = e.expansions;
     return res->status;

@@ -116,6 +116,10 @@ def test_configuration_arguments_are_checked(td):
     INVALID = td._lib.INVALID_ARG
     for bits in (-1, 1, 5, 17, 40):
         assert lib.td_configure_table(bits) == INVALID
+    for base in (-1, 1, 15):
+        assert lib.td_configure_restart(base) == INVALID
+    assert lib.td_configure_restart(0) == td._lib.OK
+    assert lib.td_configure_restart(200) == td._lib.OK
     for args in ((0, 2, 32), (1, -1, 32), (1, 9, 32), (1, 2, 0)):
         assert lib.td_configure_serve(*args) == INVALID
         assert lib.td_configure_steal(*args) == INVALID

@@ -155,3 +155,36 @@ def test_pinned_move_matches_block_swap(oracle, emu):
             cur = cur[:i] + cur[j:k] + cur[i:j] + cur[k:]
             B = [0] + [((L >> (4 * m)) & 15) + 1 for m in range(N - 1)]
             assert [B[(p + off) % N] for p in range(N)] == [sigma[a] for a in cur]
+
+
+def test_restarts_keep_verdicts_and_witnesses(oracle, emu):
+    """Free order with restarts after 16 x Luby expansions (many restarts per
+    search, each with another child order) against no restarts: the same
+    verdicts on hard S_16 instances at bound 9 and n = 13 instances at bound 6
+    (several of the latter have no witness within it, so the last, unbounded
+    attempt must search the whole tree), and every witness replays."""
+    import td16_b200 as td
+    emu.td_emu_set_restart.argtypes = [C.c_uint32]
+    cases = []
+    for seed, count, lo, hi, maxd in ((3, 24, 16, 16, 9), (5, 48, 13, 13, 6)):
+        perms, n = td.synth_perms(seed, count, lo, hi, 100, 1, 3)
+        for p, k in zip(perms, n):
+            cases.append((p[:k].tolist(), maxd))
+    statuses = {}
+    try:
+        for base in (0, 16):
+            emu.td_emu_set_restart(base)
+            out = []
+            for pi, maxd in cases:
+                beta, omega, init = oracle.perm_to_pair(pi)
+                x = _prep(emu, beta, omega, init, 0.0, maxd, True)
+                r, moves = _run(emu, x, 0)
+                if r.status == 1:
+                    abc = oracle.positions_to_symbols(beta, moves)
+                    assert oracle.validate(beta, omega, abc, maxd) is None
+                out.append(r.status)
+            statuses[base] = out
+    finally:
+        emu.td_emu_set_restart(200)
+    assert statuses[0] == statuses[16]
+    assert 0 in statuses[0] and 1 in statuses[0]

@@ -252,3 +252,27 @@ def test_explored_state_tables_keep_verdicts(slots, oracle):
     assert (tabled["status"][:200] == ost).all()
     b2, o2, _, N2 = _pairs(oracle, perms, n)
     _replay_all(oracle, b2, o2, N2, tabled, maxd)
+
+
+def test_restarts_keep_verdicts(slots, oracle):
+    """Free-order restarts (another child order after 16 x Luby expansions,
+    many per search here) against none: identical verdicts on hard S_16 at
+    bound 9 and n = 13 at bound 6 (many without a witness, searched to the
+    end by the last attempt); every witness replays."""
+    td = slots
+    p1, n1 = td.synth_perms(3, 2048, 16, 16, 100, 1, 4)
+    p2, n2 = td.synth_perms(5, 2048, 13, 13, 100, 1, 3)
+    sets = [(p1, n1, 9), (p2, n2, 6)]
+    try:
+        for perms, n, maxd in sets:
+            inst = td.prepare_perms(perms, n, maxd)
+            td._lib.configure_restart(0)
+            plain, _ = td.search_batch(0, inst, 0)
+            td._lib.configure_restart(16)
+            restarted, st = td.search_batch(0, inst, 0)
+            assert (plain["status"] == restarted["status"]).all() and st.errors == 0
+            b, o, _, N = _pairs(oracle, perms, n)
+            _replay_all(oracle, b, o, N, restarted, maxd)
+        assert (plain["status"] == 0).any()
+    finally:
+        td._lib.configure_restart(200)
