@@ -860,7 +860,11 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
                     break;
                 }
                 hungry = __shfl_sync(TD_FULL, hungry, 0);
-                if (hungry > 0) td_donate(s, *dc, code, d0, level, N, min(hungry, dc->grain));
+                // a search that has handed out subtrees no longer restarts: the
+                // subtrees of an abandoned attempt would go on being searched,
+                // and searching in parallel already varies the order
+                if (hungry > 0 && td_donate(s, *dc, code, d0, level, N, min(hungry, dc->grain)) > 0)
+                    attempt_budget = ~0u;
             }
         }
         if ((r.expansions & 255u) == 0) {
