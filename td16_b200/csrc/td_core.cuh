@@ -241,6 +241,15 @@ TD_HD uint32_t td_pair_code(int N, int q) {
     return (uint32_t)i | ((uint32_t)j << 5) | ((uint32_t)j << 10) | ((uint32_t)(31 - j) << 15);
 }
 
+// Key of a pinned state in the tables of explored states: L with its nibbles
+// from N-1 on cleared.  The first 14 nibbles and whether nibble 14 exceeds
+// nibble 15 determine it (the two are the values left over by a permutation
+// of 0..15; for N <= 16 nibble 15 is cleared), so it fits in 57 bits.
+TD_HD uint64_t td_tt_key(uint64_t L) {
+    const uint64_t order = ((L >> 56) & 15u) > ((L >> 60) & 15u) ? 1ull : 0ull;
+    return (L & 0x00ffffffffffffffull) | (order << 56);
+}
+
 // ---- restarts of the free order ----------------------------------------------
 //
 // The free-order search has a heavy tail: on near-reverse S_16 the median

@@ -52,7 +52,7 @@ struct td_warp_smem {
             uint4 rows[TD_MAX_N];
             uint2 flg[TD_MAX_N];
             // per level and lane: the expandable children of the lane's four
-            // pair slots (word r = slot 4*lane + r), +2 class at bits k-1
+            // pair slots (word r = slot R*lane + r), +2 class at bits k-1
             // (1..15), 0 class at bits k+15 (17..31)
             uint4 pw[TD_MAX_DEPTH][32];
             uint32_t m2[TD_MAX_DEPTH];                 // per level: lanes that hold +2 children
@@ -731,17 +731,19 @@ __device__ __forceinline__ int td_donate(td_warp_smem &s, const td_donate_ctx &d
 // ancestor still being explored (which has more budget) or its children were
 // donated (then their takers explore them).  The search stops at the first
 // witness, so every completed entry is a state without one.  An entry is one
-// word: the low 15 nibbles of L (the 16th is the missing value of the
-// permutation) and the depth in the top nibble.  The table is cleared at the
-// start of each unit, since the rate masks and the bound belong to the
-// instance.
+// word: the state (td_tt_key, 57 bits), a 3-bit generation and the depth in
+// the top nibble.  A unit clears its table before first use, since the rate
+// masks and the bound belong to the instance.  A restart abandons the entries
+// (their subtrees were not all searched) by moving to the next generation;
+// the table is cleared again only when the generations wrap around.
 
 #define TD_TT_EMPTY 0xffffffffffffffffull  // no state has fifteen nibbles of 15
 // A unit starts using its table after this many expansions: most searches of
 // uniform permutations end sooner, and then clearing the table would cost
 // more than it saves.  States expanded before are simply not recorded.
 #define TD_TT_AFTER 32
-#define TD_TT_LOW60 0x0fffffffffffffffull
+#define TD_TT_KEY 0x01ffffffffffffffull  // bits 0-56 of an entry: the state
+#define TD_TT_GENS 8                       // generations per clear (bits 57-59)
 
 __device__ __forceinline__ void td_tt_clear(const td_search_limits &lim) {
     const int lane = threadIdx.x & 31;
@@ -751,9 +753,11 @@ __device__ __forceinline__ void td_tt_clear(const td_search_limits &lim) {
     __syncwarp();
 }
 
-// Looks up the state of level `lv` (depth lv) and records it; returns whether
-// it was already explored at a depth <= lv (uniform across the warp).
-__device__ __forceinline__ bool td_tt_visit(const td_warp_smem &s, const td_search_limits &lim, int lv, int N) {
+// Looks up the state of level `lv` (depth lv) in generation `gen` of the table
+// and records it there; returns whether it was already explored in this
+// generation at a depth <= lv (uniform across the warp).
+__device__ __forceinline__ bool td_tt_visit(const td_warp_smem &s, const td_search_limits &lim, int lv, int N,
+                                            uint32_t gen) {
     const int m = threadIdx.x & 31;
     const int a = m < N ? s.A[lv][m] : 0xff;
     const int c0 = __ffs(__ballot_sync(TD_FULL, a == 0)) - 1;  // caller position of label 0
@@ -768,13 +772,14 @@ __device__ __forceinline__ bool td_tt_visit(const td_warp_smem &s, const td_sear
     }
     lo = __reduce_or_sync(TD_FULL, lo);
     hi = __reduce_or_sync(TD_FULL, hi);
-    const uint64_t key = ((((uint64_t)hi) << 32) | lo) & TD_TT_LOW60;
+    const uint64_t key = td_tt_key((((uint64_t)hi) << 32) | lo);
+    const uint64_t tag = key | ((uint64_t)gen << 57);
     int hit = 0;
     if (m == 0) {
         const uint32_t h = (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> (64 - lim.tt_bits));
         const uint64_t old = lim.tt[h];
-        hit = (old & TD_TT_LOW60) == key && (int)(old >> 60) <= lv;
-        if (!hit) lim.tt[h] = key | ((uint64_t)lv << 60);
+        hit = (old & (TD_TT_KEY | (7ull << 57))) == tag && (int)(old >> 60) <= lv;
+        if (!hit) lim.tt[h] = tag | ((uint64_t)lv << 60);
     }
     return __shfl_sync(TD_FULL, hit, 0) != 0;
 }
@@ -811,6 +816,7 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
     r.expansions = 1;
     int since_check = 0;
     bool tt_on = false;  // the table is in use (free order, after TD_TT_AFTER expansions)
+    uint32_t tt_gen = 0;  // its current generation
     int attempt = 0;     // free order: restarts with another child order (td_attempt_budget)
     uint32_t ord = 0, attempt_exp = 1;
     uint32_t attempt_budget = ORDERED ? ~0u : td_attempt_budget(lim.restart_base, 0);
@@ -834,7 +840,7 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
                 ord = td_order_variant(attempt);
                 attempt_budget = td_attempt_budget(lim.restart_base, attempt);
                 attempt_exp = 1;
-                tt_on = false;
+                if (tt_on && (tt_gen = (tt_gen + 1) % TD_TT_GENS) == 0) tt_on = false;  // wrapped: clear
                 level = d0;
                 const int odd = td_prepare_rows(s, d0, N, O, F);
                 found = td_evaluate_rows(s, code, N, d0, odd, O, F);
@@ -910,7 +916,7 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
                         td_tt_clear(lim);
                         tt_on = true;
                     }
-                    if (tt_on && td_tt_visit(s, lim, level + 1, N)) continue;  // explored with at least this budget
+                    if (tt_on && td_tt_visit(s, lim, level + 1, N, tt_gen)) continue;  // explored with at least this budget
                 }
                 break;
             }

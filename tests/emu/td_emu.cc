@@ -252,25 +252,28 @@ int next_child(Emu &e, int level, int *accepted) {
 }
 
 // The kernel's table of explored states (free order): 2^12 entries, key =
-// the low 15 nibbles of the pinned state (nibbles from N-1 on cleared), depth
-// in the top nibble, direct-mapped by a multiplicative hash.
+// td_tt_key of the pinned state (nibbles from N-1 on cleared), a 3-bit
+// generation, the depth in the top nibble, direct-mapped by a multiplicative
+// hash.
 #define EMU_TT_BITS 12
 // restart budget base of the free order (the kernel's default); 0 = none
 static uint32_t g_restart_base = 200;
 extern "C" void td_emu_set_restart(uint32_t base) { g_restart_base = base; }
-bool tt_visit(uint64_t *tt, uint64_t L, int N, int lv) {
+bool tt_visit(uint64_t *tt, uint64_t L, int N, int lv, uint32_t gen) {
     const uint64_t data = N - 1 >= 16 ? ~0ull : ((1ull << (4 * (N - 1))) - 1ull);
-    const uint64_t key = L & data & 0x0fffffffffffffffull;
+    const uint64_t key = td_tt_key(L & data);
+    const uint64_t tag = key | ((uint64_t)gen << 57);
     const unsigned h = (unsigned)((key * 0x9E3779B97F4A7C15ull) >> (64 - EMU_TT_BITS));
     const uint64_t old = tt[h];
-    if ((old & 0x0fffffffffffffffull) == key && (int)(old >> 60) <= lv) return true;
-    tt[h] = key | ((uint64_t)lv << 60);
+    if ((old & (0x01ffffffffffffffull | (7ull << 57))) == tag && (int)(old >> 60) <= lv) return true;
+    tt[h] = tag | ((uint64_t)lv << 60);
     return false;
 }
 
 int search_rows(Emu &e, td_result *res) {
     static thread_local uint64_t tt[1 << EMU_TT_BITS];
     bool tt_on = false;  // in use after 32 expansions, as in the kernel
+    uint32_t tt_gen = 0;
     int attempt = 0;     // restarts, as in the kernel
     uint32_t ord = 0, attempt_exp = 1, attempt_budget = td_attempt_budget(g_restart_base, 0);
     const int NP = (e.N - 1) * (e.N - 2) / 2;
@@ -293,7 +296,7 @@ int search_rows(Emu &e, td_result *res) {
             ord = td_order_variant(attempt);
             attempt_budget = td_attempt_budget(g_restart_base, attempt);
             attempt_exp = 1;
-            tt_on = false;
+            if (tt_on && (tt_gen = (tt_gen + 1) % 8) == 0) tt_on = false;  // wrapped: clear
             level = 0;
             odd = prepare_rows(e, e.L[0], e.off[0]);
             found = evaluate_rows(e, 0, odd);
@@ -313,7 +316,7 @@ int search_rows(Emu &e, td_result *res) {
             for (int q = 0; q < (1 << EMU_TT_BITS); ++q) tt[q] = ~0ull;
             tt_on = true;
         }
-        if (tt_on && tt_visit(tt, e.L[level + 1], e.N, level + 1)) continue;  // explored with at least this budget
+        if (tt_on && tt_visit(tt, e.L[level + 1], e.N, level + 1, tt_gen)) continue;  // explored with at least this budget
         ++level;
         odd = prepare_rows(e, e.L[level], e.off[level]);
         found = evaluate_rows(e, level, odd);
