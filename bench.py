@@ -41,14 +41,14 @@ WORKLOAD = "full-size decision search: 2^20 S_16 perms, 50% uniform / 50% revers
 # Per node expansion at N = 17, the search kernel's warp instructions (all
 # pipes) and those of the integer ALU pipe, and its DRAM bytes per launch:
 # ncu capture of td_steal_kernel on the first 2^18 instances of this workload
-# (tuned launch shape, explored-state tables on), summarised in
-# profiles/td_steal_kernel_s16_mix_2p18.md: 48.197 G warp instructions over
-# 55.299 M expansions (skipped children, donation and scheduling included);
-# the ALU pipe busy 71.312% of 2 warp instructions per cycle over 17.614 G SM
-# cycles; 5.43 GB of DRAM traffic, mostly the explored-state tables.
-INST_PER_EXPANSION = 48.197e9 / 55.299e6
-ALU_INST_PER_EXPANSION = 0.71312 * 2 * 17.614e9 / 55.299e6
-DRAM_BYTES_PER_2P18_LAUNCH = 5.43e9
+# (tuned launch shape, restarts and explored-state tables on), summarised in
+# profiles/td_steal_kernel_s16_mix_2p18.md: 16.293 G warp instructions over
+# 21.279 M expansions (skipped children, restarts, donation and scheduling
+# included); the ALU pipe busy 56.572% of 2 warp instructions per cycle over
+# 7.619 G SM cycles; 3.12 GB of DRAM traffic, mostly the explored-state tables.
+INST_PER_EXPANSION = 16.293e9 / 21.279e6
+ALU_INST_PER_EXPANSION = 0.56572 * 2 * 7.619e9 / 21.279e6
+DRAM_BYTES_PER_2P18_LAUNCH = 3.12e9
 
 def rank_info():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
