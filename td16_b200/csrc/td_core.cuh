@@ -288,6 +288,15 @@ TD_HD uint32_t td_order_variant(int a) {
     return ((uint32_t)(7 * a) & 31u) | (((uint32_t)a & 1u) << 5) | ((((uint32_t)a >> 1) & 1u) << 6);
 }
 
+// The order at DFS level `level` of attempt a: the rotation also moves by
+// 11 x level x a, so that the levels of one attempt do not all favour the
+// same lanes (in the host emulation this halved the mean expansions of
+// near-reverse S_16 searches against one rotation per attempt).
+TD_HD uint32_t td_level_order(uint32_t ord, int a, int level) {
+    if (a == 0) return 0u;
+    return (ord & ~31u) | ((ord + 11u * (uint32_t)level * (uint32_t)a) & 31u);
+}
+
 // Per-position cycle descriptor: leader (smallest pinned position of the
 // cycle), dist (omega steps to the leader), len (cycle length).
 TD_HD uint32_t td_pair_entry(int leader_p, int dist_p, int len_p, int leader_q,

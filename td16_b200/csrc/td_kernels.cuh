@@ -902,7 +902,7 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
                 if (accepted) walk = 2;
                 break;
             } else {
-                const int m = td_next_child_rows(s, code, level, ord);
+                const int m = td_next_child_rows(s, code, level, td_level_order(ord, attempt, level));
                 if (m < 0) {
                     if (level == d0) { walk = 1; break; }
                     --level;

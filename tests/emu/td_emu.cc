@@ -302,7 +302,7 @@ int search_rows(Emu &e, td_result *res) {
             found = evaluate_rows(e, 0, odd);
             continue;
         }
-        const int t = next_child_rows(e, level, ord);
+        const int t = next_child_rows(e, level, td_level_order(ord, attempt, level));
         if (t < 0) {
             if (level == 0) { res->status = TD_NOT_FOUND; break; }
             --level;
