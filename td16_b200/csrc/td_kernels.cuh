@@ -30,7 +30,6 @@
 #define TD_TRI_TABLE 3060      // sum over N <= 17 of C(N,3) = C(18,4)
 #define TD_G0 0x09249249u      // bit 0 of each 3-bit group
 #define TD_G1 0x12492492u      // bit 1 of each group
-#define TD_G2 0x24924924u      // bit 2 of each group
 
 // floor(b / 3) for 0 <= b <= 29: the step of a bit inside a packed word
 __device__ __forceinline__ int td_group_of(int b) { return (b * 11) >> 5; }
@@ -42,8 +41,7 @@ struct td_warp_smem {
             uint8_t pt[TD_PT_ROWS * TD_PT_STRIDE];     // pair table of the current node
             // per level, per lane: the outcome of every step in 3-bit groups, ten
             // steps per word (step st in word st/10 at bit 3*(st%10)): bit 0 found
-            // (accepted root in ordered mode), bit 1 first-choice child, bit 2
-            // second-choice child
+            // (or, at the root level, accepted when visited), bit 1 a child to visit
             uint32_t pm[TD_MAX_DEPTH][3][32];
         };
         struct {  // free move order (bit-sliced: one pair and all its k per lane and round)
@@ -225,9 +223,8 @@ __device__ __forceinline__ uint64_t td_globaltimer() {
     return t;
 }
 
-// Evaluate all children of the node at `level`.  Fills the level's packed
-// outcome words and returns the found child's u, or -1.
-template <bool ORDERED>
+// Reference order: evaluate all children of the node at `level`.  Fills the
+// level's packed outcome words and returns the found child's u, or -1.
 __device__ __forceinline__ int td_evaluate(td_warp_smem &s, const uint8_t *lut,
                                            const uint32_t (&code)[TD_MAX_STEPS], int steps,
                                            int level, int odd, int maxd) {
@@ -238,7 +235,7 @@ __device__ __forceinline__ int td_evaluate(td_warp_smem &s, const uint8_t *lut,
     const uint32_t x0 = ((reachD >> odd) & 1u) & (f0 ^ 1u);
     const uint32_t x2 = ((reachD >> (odd + 2)) & 1u) & (f2 ^ 1u);
     // byte c of nt holds the flags of class c; byte 0 (filtered out) is zero
-    const uint32_t flags0 = ORDERED ? (f0 | (x0 << 1)) : (f0 | (x0 << 2));
+    const uint32_t flags0 = f0 | (x0 << 1);
     const uint32_t flags2 = f2 | (x2 << 1);
     const uint32_t nt = (flags0 << (8 * TD_CLASS_ZERO)) | (flags2 << (8 * TD_CLASS_PLUS2));
     (void)maxd;
@@ -262,7 +259,7 @@ __device__ __forceinline__ int td_evaluate(td_warp_smem &s, const uint8_t *lut,
     s.pm[level][0][lane] = P0;
     s.pm[level][1][lane] = P1;
     s.pm[level][2][lane] = P2;
-    if (ORDERED && level == 0) return -1;  // roots are accepted on visit, not on seeding
+    if (level == 0) return -1;  // roots are accepted on visit, not on seeding
     const uint32_t q0 = P0 & TD_G0, q1 = P1 & TD_G0, q2 = P2 & TD_G0;
     if (__any_sync(TD_FULL, (q0 | q1 | q2) != 0)) {
         int st = -1;
@@ -275,20 +272,13 @@ __device__ __forceinline__ int td_evaluate(td_warp_smem &s, const uint8_t *lut,
     return -1;
 }
 
-// Next child of `level`; returns u or -1.  *accepted is set for a root that
-// is accepted when visited (ordered mode).
-template <bool ORDERED>
+// Reference order: next child of `level`; returns u or -1.  *accepted is set
+// for a root that is accepted when visited.
 __device__ __forceinline__ int td_next_child(td_warp_smem &s, int level, int *accepted) {
     const int lane = threadIdx.x & 31;
     const uint32_t P0 = s.pm[level][0][lane], P1 = s.pm[level][1][lane], P2 = s.pm[level][2][lane];
-    const bool desc_lanes = ORDERED && level > 0;
-    uint32_t cm;
-    if (ORDERED) {
-        cm = level == 0 ? (TD_G0 | TD_G1) : TD_G1;
-    } else {
-        const bool any1 = __any_sync(TD_FULL, ((P0 | P1 | P2) & TD_G1) != 0);
-        cm = any1 ? TD_G1 : TD_G2;  // +2 children first
-    }
+    const bool desc_lanes = level > 0;
+    const uint32_t cm = level == 0 ? (TD_G0 | TD_G1) : TD_G1;
     const uint32_t w0 = P0 & cm, w1 = P1 & cm, w2 = P2 & cm;
     int st = -1;
     if (w2) st = 20 + td_group_of(31 - __clz(w2));
@@ -305,7 +295,7 @@ __device__ __forceinline__ int td_next_child(td_warp_smem &s, int level, int *ac
     const int k = st < 10 ? 0 : (st < 20 ? 1 : 2);
     const int j = st - 10 * k;
     const uint32_t Pk = k == 0 ? P0 : (k == 1 ? P1 : P2);
-    if (ORDERED && level == 0) *accepted = __shfl_sync(TD_FULL, (int)((Pk >> (3 * j)) & 1u), win);
+    if (level == 0) *accepted = __shfl_sync(TD_FULL, (int)((Pk >> (3 * j)) & 1u), win);
     if (lane == win) s.pm[level][k][lane] = Pk & ~(7u << (3 * j));
     __syncwarp();
     return st * 32 + win;
@@ -806,7 +796,7 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
     int found;
     if constexpr (ORDERED) {
         const int odd = td_prepare_node(s, s.L[d0], s.off[d0], N);
-        found = td_evaluate<true>(s, lut, code, steps, d0, odd, maxd);
+        found = td_evaluate(s, lut, code, steps, d0, odd, maxd);
         if (found >= 0) found = td_tri_table[tri_base + T - 1 - found];
     } else {
         td_unpack_state(s, d0, s.L[d0], s.off[d0], N);
@@ -892,7 +882,7 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
         for (;;) {
             if constexpr (ORDERED) {
                 int accepted;
-                const int u = td_next_child<true>(s, level, &accepted);
+                const int u = td_next_child(s, level, &accepted);
                 if (u < 0) {
                     if (level == d0) { walk = 1; break; }
                     --level;
@@ -940,7 +930,7 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
             }
             ++level;
             const int odd = td_prepare_node(s, nL, noff, N);
-            found = td_evaluate<true>(s, lut, code, steps, level, odd, maxd);
+            found = td_evaluate(s, lut, code, steps, level, odd, maxd);
             if (found >= 0) found = td_tri_table[tri_base + T - 1 - found];
         } else {
             ++level;

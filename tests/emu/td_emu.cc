@@ -1,10 +1,15 @@
 // td_emu.cc -- serial host emulation of the engine's warp algorithm.
 //
-// TEST INFRASTRUCTURE ONLY.  It runs the kernel's exact per-node steps
-// (pinned state, pair table, 12-bit class table, per-lane step bitmasks,
-// child selection order) one lane at a time, so the CPU test suite can check
-// the engine's logic against the oracle without a GPU.  The product library
-// does not contain or call it.
+// TEST INFRASTRUCTURE ONLY.  It runs the kernel's per-node steps one lane at a
+// time, so the CPU test suite can check the engine's logic against the oracle
+// without a GPU:
+//   reference order: pinned state, pair table, 12-bit class table, per-lane
+//     step bitmasks and the single-queue child order;
+//   free order: row masks and bit-sliced classes (td_row_classes), pair slots,
+//     the +2-first child order, the table of explored states and the restarts
+//     with their child orders (td_attempt_budget, td_level_order).
+// It shares the kernel's helpers in td_core.cuh.  The product library does not
+// contain or call it.
 #include "../../td16_b200/csrc/td_core.cuh"
 
 #include <string.h>
