@@ -338,6 +338,36 @@ __global__ void td_epoch_kernel(uint32_t *epoch) {
     *epoch = e ? e : 1;
 }
 
+// The totals of td_batch_stats, reduced on the device so that the host does
+// not walk the result array (2^20 results are 32 MiB of host memory).  Reads
+// only the status and expansion words of each record.
+struct td_counts {
+    unsigned long long expansions, found, not_found, errors;
+};
+
+__global__ void __launch_bounds__(256) td_count_kernel(const td_result *__restrict__ res, int count,
+                                                       td_counts *__restrict__ c) {
+    unsigned long long e = 0;
+    uint32_t f = 0, nf = 0, er = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const int st = res[i].status;
+        e += res[i].expansions;
+        f += st == TD_FOUND;
+        nf += st == TD_NOT_FOUND;
+        er += st != TD_FOUND && st != TD_NOT_FOUND;
+    }
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(TD_FULL, e, o);
+    f = __reduce_add_sync(TD_FULL, f);
+    nf = __reduce_add_sync(TD_FULL, nf);
+    er = __reduce_add_sync(TD_FULL, er);
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&c->expansions, e);
+        atomicAdd(&c->found, (unsigned long long)f);
+        atomicAdd(&c->not_found, (unsigned long long)nf);
+        atomicAdd(&c->errors, (unsigned long long)er);
+    }
+}
+
 // Witness replay in pinned form: every move must be an in-range position
 // triple i<j<k, at most max_moves of them, and the final state must be the
 // identity (omega = id  <=>  beta = rho  <=>  L = 0,1,...,n-1).
@@ -427,6 +457,12 @@ struct Slot {
     td_inst_state *d_state = nullptr;
     size_t state_count = 0;
     uint32_t *d_epoch = nullptr;
+    // td_batch_stats of host-buffer batches: device totals and their pinned copy
+    td_counts *d_counts = nullptr;
+    struct HostStats {
+        td_counts counts;
+        td_pool pool;
+    } *h_stats = nullptr;
     int slots_on_device = 1;
     std::mutex *mu = nullptr;
 };
@@ -533,6 +569,8 @@ void release_slot(Slot &s) {
     if (s.d_tt) cudaFree(s.d_tt);
     if (s.d_epoch) cudaFree(s.d_epoch);
     if (s.d_state) cudaFree(s.d_state);
+    if (s.d_counts) cudaFree(s.d_counts);
+    if (s.h_stats) cudaFreeHost(s.h_stats);
     if (s.h_inst) cudaFreeHost(s.h_inst);
     if (s.h_res) cudaFreeHost(s.h_res);
     if (s.done) cudaEventDestroy(s.done);
@@ -1037,6 +1075,10 @@ TD_API int td_search_batch(int slot, int count, const td_instance *in, td_result
         set_err(err, errlen, "invalid batch arguments");
         return TD_INVALID_ARG;
     }
+    if (count == 0) {
+        if (stats) std::memset(stats, 0, sizeof *stats);
+        return TD_OK;
+    }
     std::lock_guard<std::mutex> g(*s->mu);
     TD_CHECK(cudaSetDevice(s->device));
     const size_t need = (size_t)count * (sizeof(td_instance) + sizeof(td_result));
@@ -1047,6 +1089,10 @@ TD_API int td_search_batch(int slot, int count, const td_instance *in, td_result
         TD_CHECK(cudaMalloc(&s->d_batch, need));
         s->d_batch_bytes = need;
     }
+    if (stats && !s->d_counts) {
+        TD_CHECK(cudaMalloc(&s->d_counts, sizeof(td_counts)));
+        TD_CHECK(cudaMallocHost(&s->h_stats, sizeof(Slot::HostStats)));
+    }
     td_instance *d_in = (td_instance *)s->d_batch;
     td_result *d_out = (td_result *)((char *)s->d_batch + (size_t)count * sizeof(td_instance));
     TD_CHECK(cudaMemcpyAsync(d_in, in, (size_t)count * sizeof(td_instance), cudaMemcpyHostToDevice, s->stream));
@@ -1054,15 +1100,26 @@ TD_API int td_search_batch(int slot, int count, const td_instance *in, td_result
     int rc = launch_batch(*s, count, d_in, d_out, flags, max_exp, s->stream, err, errlen);
     if (rc != TD_OK) return rc;
     TD_CHECK(cudaEventRecord(s->t1, s->stream));
+    const bool pooled = !(flags & (TD_FLAG_ORDERED | TD_FLAG_PLAIN)) && s->d_pool;
+    if (stats) {
+        TD_CHECK(cudaMemsetAsync(s->d_counts, 0, sizeof(td_counts), s->stream));
+        const int blocks = std::max(1, std::min((count + 255) / 256, g_dev[s->device].sms * 8));
+        td_count_kernel<<<blocks, 256, 0, s->stream>>>(d_out, count, s->d_counts);
+        TD_CHECK(cudaGetLastError());
+        TD_CHECK(cudaMemcpyAsync(&s->h_stats->counts, s->d_counts, sizeof(td_counts), cudaMemcpyDeviceToHost,
+                                 s->stream));
+        if (pooled)
+            TD_CHECK(cudaMemcpyAsync(&s->h_stats->pool, s->d_pool, sizeof(td_pool), cudaMemcpyDeviceToHost,
+                                     s->stream));
+    }
     TD_CHECK(cudaMemcpyAsync(out, d_out, (size_t)count * sizeof(td_result), cudaMemcpyDeviceToHost, s->stream));
     TD_CHECK(cudaEventRecord(s->done, s->stream));
     TD_CHECK(cudaEventSynchronize(s->done));
     if (stats) {
         std::memset(stats, 0, sizeof *stats);
         TD_CHECK(cudaEventElapsedTime(&stats->kernel_ms, s->t0, s->t1));
-        if (!(flags & (TD_FLAG_ORDERED | TD_FLAG_PLAIN)) && s->d_pool) {
-            td_pool pool;
-            TD_CHECK(cudaMemcpy(&pool, s->d_pool, sizeof pool, cudaMemcpyDeviceToHost));
+        if (pooled) {
+            const td_pool &pool = s->h_stats->pool;
             stats->donations = pool.donations;
             stats->donated_items = pool.donated_items;
             if (pool.error) {
@@ -1070,12 +1127,11 @@ TD_API int td_search_batch(int slot, int count, const td_instance *in, td_result
                 return TD_TIMEOUT;
             }
         }
-        for (int i = 0; i < count; ++i) {
-            stats->expansions += out[i].expansions;
-            if (out[i].status == TD_FOUND) stats->found++;
-            else if (out[i].status == TD_NOT_FOUND) stats->not_found++;
-            else stats->errors++;
-        }
+        const td_counts &c = s->h_stats->counts;
+        stats->expansions = c.expansions;
+        stats->found = c.found;
+        stats->not_found = c.not_found;
+        stats->errors = c.errors;
     }
     return TD_OK;
 }

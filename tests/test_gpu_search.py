@@ -276,3 +276,23 @@ def test_restarts_keep_verdicts(slots, oracle):
         assert (plain["status"] == 0).any()
     finally:
         td._lib.configure_restart(200)
+
+
+def test_batch_stats_match_the_results(slots):
+    """td_batch_stats totals (reduced on the device) equal the sums over the
+    returned records, in every launch form, with and without per-instance
+    budget errors."""
+    td = slots
+    perms, n = td.synth_perms(11, 3000, 9, 13, 50, 1, 3)
+    inst = td.prepare_perms(perms, n, (n // 2 + 1).astype(np.int32))
+    for flags, budget in ((0, 0), (ORDERED, 0), (PLAIN, 0), (0, 2), (ORDERED, 2)):
+        res, st = td.search_batch(1, inst, flags, max_expansions=budget)
+        status = res["status"]
+        assert st.found == int((status == 1).sum())
+        assert st.not_found == int((status == 0).sum())
+        assert st.errors == int(((status != 0) & (status != 1)).sum())
+        assert st.expansions == int(res["expansions"].astype(np.uint64).sum())
+        if budget:
+            assert st.errors > 0
+    empty, st = td.search_batch(1, inst[:0], 0)
+    assert len(empty) == 0 and st.found == st.not_found == st.errors == st.expansions == 0
