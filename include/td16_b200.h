@@ -160,7 +160,12 @@ int td_synth_perms(uint64_t seed, int count, int n_min, int n_max, int hard_pct,
 
 /* ---- batch search -------------------------------------------------------- */
 
-/* Host buffers in and out; copies, launches and waits on the slot's stream. */
+/* Host buffers in and out; copies, launches and waits on the slot's stream.
+ * max_expansions (all batch forms): 0 = no budget; otherwise a search that
+ * expands more nodes without finding a witness ends with status -2 (budget).
+ * In the free order the budget bounds each unit of work, i.e. the root search
+ * and each subtree donated to another warp.  stats may be NULL; its totals are
+ * reduced on the device. */
 int td_search_batch(int slot, int count, const td_instance *instances,
                     td_result *results, unsigned flags,
                     uint64_t max_expansions, td_batch_stats *stats, char *err,

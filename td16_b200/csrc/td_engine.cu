@@ -145,6 +145,7 @@ __device__ __forceinline__ int td_finish_unit(const td_dfs_out &r, td_inst_state
         atomicAdd(&st->expansions, r.expansions);
         if (r.status == TD_DFS_FOUND) win = atomicCAS(&st->found, 0, 1) == 0;
         if (r.status == TD_DFS_TIMEOUT) atomicCAS(&st->error, 0, TD_ERR_TIMEOUT);
+        if (r.status == TD_DFS_BUDGET) atomicCAS(&st->error, 0, TD_ERR_BUDGET);
     }
     win = __shfl_sync(TD_FULL, win, 0);
     if (win) td_write_result(out, TD_FOUND, r.depth, r.found_move, path, 0, 0, 7);
@@ -181,7 +182,8 @@ __global__ void __launch_bounds__(256, TD_STEAL_MIN_BLOCKS) td_steal_kernel(cons
                                                       td_item *items, uint32_t *ready, const uint32_t *epoch_ptr,
                                                       int capacity, td_inst_state *state, int grain,
                                                       int max_level, int check_every, uint64_t time_limit_ns,
-                                                      uint64_t *tt, int tt_bits, uint32_t restart_base) {
+                                                      uint64_t *tt, int tt_bits, uint32_t restart_base,
+                                                      uint64_t max_exp) {
     extern __shared__ __align__(16) uint8_t td_smem[];
     const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // free order only: no class table, the warp frames start the block's shared memory
@@ -191,7 +193,10 @@ __global__ void __launch_bounds__(256, TD_STEAL_MIN_BLOCKS) td_steal_kernel(cons
     td_warp_smem &s = ws[warp];
     uint32_t code[TD_MAX_STEPS];
     int codeN = -1;
-    td_search_limits lim = td_make_limits(0, time_limit_ns, nullptr);
+    // the expansion budget bounds each unit (the root search and each donated
+    // subtree); an instance without a witness whose unit ran out reports
+    // TD_ERR_BUDGET
+    td_search_limits lim = td_make_limits(max_exp, time_limit_ns, nullptr);
     lim.restart_base = restart_base;
     if (tt) {
         lim.tt = tt + ((size_t)(blockIdx.x * warps + warp) << tt_bits);
@@ -648,7 +653,7 @@ int launch_batch(Slot &s, int count, const td_instance *d_in, td_result *d_out, 
                                                                             s.d_ready, s.d_epoch,
                                                          s.item_capacity, s.d_state, g_steal_grain, g_split_level,
                                                          g_check_every, time_limit_ns(), g_tt_bits > 0 ? s.d_tt : nullptr,
-                                                         g_tt_bits, g_restart_base);
+                                                         g_tt_bits, g_restart_base, max_exp);
     } else {
         DeviceInfo &d = g_dev[s.device];
         if (d.blocks_per_sm == 0) {
@@ -1370,7 +1375,7 @@ TD_API int td_search_batch_noalloc(int count, const td_instance *d_instances, td
         const int grid = std::max(1, std::min(d.sms * std::max(1, d.steal_blocks), blocks_needed));
         td_steal_kernel<<<grid, threads, smem, st>>>(d_instances, d_results, count, pool, items, ready, epoch,
                                                      TD_NOALLOC_ITEMS, state, g_steal_grain, g_split_level,
-                                                     g_check_every, limit, nullptr, 0, g_restart_base);
+                                                     g_check_every, limit, nullptr, 0, g_restart_base, max_exp);
     }
     TD_CHECK_NA(cudaGetLastError());
     if (flags & TD_FLAG_VERIFY) {

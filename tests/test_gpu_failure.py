@@ -40,8 +40,12 @@ def test_budget_exhaustion_is_reported_per_instance(td):
     try:
         perms, n = td.synth_perms(2, 512, 16, 16, 100, 1, 4)
         inst = td.prepare_perms(perms, n, 9)
-        res, _ = td.search_batch(0, inst, td._lib.FLAG_ORDERED, max_expansions=3)
-        assert set(np.unique(res["status"]).tolist()) <= {-2, 1}
-        assert (res["status"] == -2).any()
+        for flags in (td._lib.FLAG_ORDERED, 0):  # reference order; free order (per unit of work)
+            res, _ = td.search_batch(0, inst, flags, max_expansions=3)
+            assert set(np.unique(res["status"]).tolist()) <= {-2, 1}
+            assert (res["status"] == -2).any()
+        # without a budget the same batch has no errors
+        res, _ = td.search_batch(0, inst, 0)
+        assert (res["status"] == 1).all()
     finally:
         td.destroy()
