@@ -123,6 +123,17 @@ def make_instances(td, rank, count=COUNT, workload="mix"):
     return td.prepare_perms(perms, n, MAX_MOVES), perms, n
 
 
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_baseline(seconds_target=15.0, sample=96):
     """The oracle (CPU restatement of the reference search, its single-queue
     order) on all host cores, on a bounded sample of the workload."""
@@ -149,6 +160,8 @@ def cpu_baseline(seconds_target=15.0, sample=96):
         verified += O.validate(beta[i].tolist(), omega[i].tolist(), abc, MAX_MOVES) is None
     return {"value": verified / dt, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"first {c} instances of the workload (seed {SEED}), {dt:.1f} s on {cores} threads",
+            "label": "CPU restatement of the reference algorithm (the reference has no CPU search)",
+            "nproc": os.cpu_count(), "cpu_model": cpu_model(),
             "expansions_per_s": float(ex.sum()) / dt, "seconds": dt}
 
 
@@ -171,7 +184,8 @@ def run_reference(args):
             "data": "synthetic (seeded)", "config": {"workload": WORKLOAD, "count": COUNT, "seed": SEED,
                                                      "max_moves": MAX_MOVES, "l2": "n/a (CPU)"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": res["cores"], "kind": "port",
-                             "sample": res["sample"]},
+                             "sample": res["sample"], "label": res["label"], "nproc": res["nproc"],
+                             "cpu_model": res["cpu_model"]},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
