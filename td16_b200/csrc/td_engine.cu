@@ -1094,10 +1094,8 @@ TD_API int td_search_batch(int slot, int count, const td_instance *in, td_result
         TD_CHECK(cudaMalloc(&s->d_batch, need));
         s->d_batch_bytes = need;
     }
-    if (stats && !s->d_counts) {
-        TD_CHECK(cudaMalloc(&s->d_counts, sizeof(td_counts)));
-        TD_CHECK(cudaMallocHost(&s->h_stats, sizeof(Slot::HostStats)));
-    }
+    if (stats && !s->d_counts) TD_CHECK(cudaMalloc(&s->d_counts, sizeof(td_counts)));
+    if (stats && !s->h_stats) TD_CHECK(cudaMallocHost(&s->h_stats, sizeof(Slot::HostStats)));
     td_instance *d_in = (td_instance *)s->d_batch;
     td_result *d_out = (td_result *)((char *)s->d_batch + (size_t)count * sizeof(td_instance));
     TD_CHECK(cudaMemcpyAsync(d_in, in, (size_t)count * sizeof(td_instance), cudaMemcpyHostToDevice, s->stream));
