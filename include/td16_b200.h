@@ -130,9 +130,10 @@ int td_configure_serve(int grain, int split_level, int check_every);
  * or 0 for none.  Verdicts do not depend on it. */
 int td_configure_table(int bits);
 /* Free-order batch searches restart with another child order after
- * base x 1, 1, 2, 1, 1, 2, 4, ... expansions (the Luby sequence; after 24
- * attempts the search runs to the end).  base >= 16 (default 200), or 0 for
- * no restarts.  Verdicts do not depend on it. */
+ * base x 1, 1, 2, 1, 1, 2, 4, ... expansions (the Luby sequence; after 32
+ * attempts the search runs to the end, in the first attempt's order).
+ * base >= 16 (default 16), or 0 for no restarts.  Verdicts do not depend on
+ * it. */
 int td_configure_restart(int base);
 
 /* ---- instance preparation (host, no GPU needed) -------------------------- */

@@ -7,9 +7,11 @@ launch on a sample for every point of a grid over
   split depth (deepest DFS level whose children may be donated),
   check interval (expansions between idle checks),
 and then, with the winning shape, the restart budget base of the root searches
-(0 = no restarts),
-keeps the fastest by device time, and stores the winners per bucket in
-td16_b200/tuned.json.  `apply(N)` configures the engine for a bucket.
+(0 = no restarts); when restarts win, the grid is searched again with that
+base and the base swept once more, since restarts shorten the searches that
+the donation knobs were tuned for.  The fastest point by device time is kept,
+and the winners per bucket are stored in td16_b200/tuned.json.  `apply(N)`
+configures the engine for a bucket.
 
     python -m td16_b200.autotune [--quick]
 """
@@ -37,7 +39,7 @@ GRID = {
 QUICK = {"warps": [2, 4], "grain": [4, 8], "split_level": [4], "check_every": [32, 128]}
 
 
-RESTARTS = [0, 32, 64, 128, 256]
+RESTARTS = [0, 16, 24, 32, 48, 64, 128]
 
 
 def _configure(p):
@@ -61,21 +63,31 @@ def tune_bucket(slot: int, instances: np.ndarray, grid=None, repeats: int = 2, l
     grid = grid or GRID
     keys = list(grid)
     results = []
-    for combo in itertools.product(*(grid[k] for k in keys)):
-        p = dict(zip(keys, combo))
-        ms = time_point(slot, instances, p, repeats)
-        results.append((ms, p))
-        log(f"  {p} -> {ms:.2f} ms")
-    results.sort(key=lambda r: r[0])
-    best_ms, best = results[0]
-    # then the restart budget base with the winning launch shape
-    for base in RESTARTS:
-        p = dict(best, restart=base)
-        ms = time_point(slot, instances, p, repeats)
-        results.append((ms, p))
-        log(f"  {p} -> {ms:.2f} ms")
-        if ms < best_ms:
-            best_ms, best = ms, p
+
+    def shapes(restart):
+        out = []
+        for combo in itertools.product(*(grid[k] for k in keys)):
+            p = dict(zip(keys, combo), restart=restart)
+            ms = time_point(slot, instances, p, repeats)
+            out.append((ms, p))
+            log(f"  {p} -> {ms:.2f} ms")
+        results.extend(out)
+        return min(out, key=lambda r: r[0])
+
+    def bases(best_ms, best):
+        for base in RESTARTS:
+            p = dict(best, restart=base)
+            ms = time_point(slot, instances, p, repeats)
+            results.append((ms, p))
+            log(f"  {p} -> {ms:.2f} ms")
+            if ms < best_ms:
+                best_ms, best = ms, p
+        return best_ms, best
+
+    best_ms, best = bases(*shapes(0))
+    if best["restart"]:
+        best_ms, best = min([(best_ms, best), shapes(best["restart"])], key=lambda r: r[0])
+        best_ms, best = bases(best_ms, best)
     _configure(DEFAULT)
     return {"params": best, "kernel_ms": best_ms, "points": len(results)}
 

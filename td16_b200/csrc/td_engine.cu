@@ -54,7 +54,7 @@ static_assert(sizeof(td_result) == 32, "td_result layout");
 
 #define TD_LUT_BYTES 4096
 #define TD_TT_BITS 12  // default: 4096 explored-state entries (32 KiB) per warp of a free-order launch
-#define TD_RESTART_BASE 200  // default base of the free order's restart budgets (expansions)
+#define TD_RESTART_BASE 16  // default base of the free order's restart budgets (expansions)
 
 // Class table (td_class_of_index for every 12-bit index), filled by the host.
 __device__ __align__(16) uint8_t td_lut_global[TD_LUT_BYTES];

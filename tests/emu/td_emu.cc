@@ -262,7 +262,7 @@ int next_child(Emu &e, int level, int *accepted) {
 // hash.
 #define EMU_TT_BITS 12
 // restart budget base of the free order (the kernel's default); 0 = none
-static uint32_t g_restart_base = 200;
+static uint32_t g_restart_base = 16;
 extern "C" void td_emu_set_restart(uint32_t base) { g_restart_base = base; }
 bool tt_visit(uint64_t *tt, uint64_t L, int N, int lv, uint32_t gen) {
     const uint64_t data = N - 1 >= 16 ? ~0ull : ((1ull << (4 * (N - 1))) - 1ull);
