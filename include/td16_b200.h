@@ -119,7 +119,9 @@ int td_configure(int warps_per_block, int grain);
  * 300): searches and device waits that pass it end with a timeout status. */
 int td_set_time_limit(double seconds);
 /* Work donation of the free-order engine: items per donation, deepest level
- * whose children may be donated, expansions between idle checks. */
+ * whose children may be donated, expansions between idle checks (default
+ * 4, 2, 64: the best setting for one blocking search per call; the
+ * autotuner's tuned.json holds the batch settings). */
 int td_configure_steal(int grain, int split_level, int check_every);
 /* The same for later serving launches (td_serve_open), kept apart because a
  * serving launch trades throughput for latency (default 1, 2, 32). */

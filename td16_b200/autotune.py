@@ -28,7 +28,7 @@ import numpy as np
 from . import _lib
 
 TUNED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned.json")
-DEFAULT = {"warps": 4, "grain": 4, "split_level": 4, "check_every": 8, "restart": 0}
+DEFAULT = {"warps": 4, "grain": 4, "split_level": 2, "check_every": 64, "restart": 16}  # the library's defaults
 
 GRID = {
     "warps": [4, 8],

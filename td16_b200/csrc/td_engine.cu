@@ -484,9 +484,11 @@ std::vector<DeviceInfo> g_dev;
 
 int g_warps_per_block = 4;
 int g_grain = 1;            // instances per ticket (ordered persistent kernel)
+// defaults: the best per-call setting (one blocking search per slot call,
+// 16 slots, S_16) measured from native threads; batch callers use tuned ones
 int g_steal_grain = 4;      // items per donation
-int g_split_level = 4;      // donate children of levels <= this
-int g_check_every = 8;      // expansions between idle checks
+int g_split_level = 2;      // donate children of levels <= this
+int g_check_every = 64;     // expansions between idle checks
 // the same for serving launches, where latency rather than throughput counts
 int g_serve_grain = 1;
 int g_serve_split_level = 2;
