@@ -42,13 +42,13 @@ WORKLOAD = "full-size decision search: 2^20 S_16 perms, 50% uniform / 50% revers
 # pipes) and those of the integer ALU pipe, and its DRAM bytes per launch:
 # ncu capture of td_steal_kernel on the first 2^18 instances of this workload
 # (tuned launch shape, restarts and explored-state tables on), summarised in
-# profiles/td_steal_kernel_s16_mix_2p18.md: 11.349 G warp instructions over
-# 14.65 M expansions (skipped children, restarts, donation and scheduling
-# included); the ALU pipe busy 59.556% of 2 warp instructions per cycle over
-# 5.175 G SM cycles; 2.25 GB of DRAM traffic, mostly the explored-state tables.
-INST_PER_EXPANSION = 11.349e9 / 14.65e6
-ALU_INST_PER_EXPANSION = 0.59556 * 2 * 5.175e9 / 14.65e6
-DRAM_BYTES_PER_2P18_LAUNCH = 2.25e9
+# profiles/td_steal_kernel_s16_mix_2p18.md: 10.892 G warp instructions over
+# 14.18 M expansions (skipped children, restarts, donation and scheduling
+# included); the ALU pipe busy 55.413% of 2 warp instructions per cycle over
+# 5.262 G SM cycles; 2.01 GB of DRAM traffic, mostly the explored-state tables.
+INST_PER_EXPANSION = 10.892e9 / 14.18e6
+ALU_INST_PER_EXPANSION = 0.55413 * 2 * 5.262e9 / 14.18e6
+DRAM_BYTES_PER_2P18_LAUNCH = 2.01e9
 
 def rank_info():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
