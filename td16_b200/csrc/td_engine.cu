@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(256, TD_STEAL_MIN_BLOCKS) td_steal_kernel(cons
                                                       int capacity, td_inst_state *state, int grain,
                                                       int max_level, int check_every, uint64_t time_limit_ns,
                                                       uint64_t *tt, int tt_bits, uint32_t restart_base,
-                                                      uint64_t max_exp) {
+                                                      uint64_t max_exp, unsigned max_backoff_ns) {
     extern __shared__ __align__(16) uint8_t td_smem[];
     const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // free order only: no class table, the warp frames start the block's shared memory
@@ -255,10 +255,13 @@ __global__ void __launch_bounds__(256, TD_STEAL_MIN_BLOCKS) td_steal_kernel(cons
                 }
             }
             if (__shfl_sync(TD_FULL, done, 0)) break;
-            // waiting warps back off to 32 us so that their counter reads do
-            // not crowd the L2 slices the busy warps' atomics go to
+            // waiting warps back off (to 32 us in a batch) so that their
+            // counter reads do not crowd the L2 slices the busy warps'
+            // atomics go to; a single search (one per call) caps it lower,
+            // since there the launch ends only when every waiting warp has
+            // woken up and seen that the work is done
             __nanosleep(backoff);
-            backoff = min(backoff * 2u, 32768u);
+            backoff = min(backoff * 2u, max_backoff_ns);
             continue;
         }
         if (lane == 0 && idle) { atomicSub(&pool->idle, 1); idle = false; }
@@ -654,7 +657,8 @@ int launch_batch(Slot &s, int count, const td_instance *d_in, td_result *d_out, 
                                                                             s.d_ready, s.d_epoch,
                                                          s.item_capacity, s.d_state, g_steal_grain, g_split_level,
                                                          g_check_every, time_limit_ns(), g_tt_bits > 0 ? s.d_tt : nullptr,
-                                                         g_tt_bits, g_restart_base, max_exp);
+                                                         g_tt_bits, g_restart_base, max_exp,
+                                                         count == 1 ? 4096u : 32768u);
     } else {
         DeviceInfo &d = g_dev[s.device];
         if (d.blocks_per_sm == 0) {
@@ -1374,7 +1378,7 @@ TD_API int td_search_batch_noalloc(int count, const td_instance *d_instances, td
         const int grid = std::max(1, std::min(d.sms * std::max(1, d.steal_blocks), blocks_needed));
         td_steal_kernel<<<grid, threads, smem, st>>>(d_instances, d_results, count, pool, items, ready, epoch,
                                                      TD_NOALLOC_ITEMS, state, g_steal_grain, g_split_level,
-                                                     g_check_every, limit, nullptr, 0, g_restart_base, max_exp);
+                                                     g_check_every, limit, nullptr, 0, g_restart_base, max_exp, 32768u);
     }
     TD_CHECK_NA(cudaGetLastError());
     if (flags & TD_FLAG_VERIFY) {
