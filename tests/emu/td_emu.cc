@@ -264,6 +264,11 @@ int next_child(Emu &e, int level, int *accepted) {
 // restart budget base of the free order (the kernel's default); 0 = none
 static uint32_t g_restart_base = 16;
 extern "C" void td_emu_set_restart(uint32_t base) { g_restart_base = base; }
+// The child order at DFS level `level` of attempt a, its budget for a base,
+// and the number of budgeted attempts (td_core.cuh), for the CPU tests.
+extern "C" uint32_t td_emu_order(int a, int level) { return td_level_order(td_order_variant(a), a, level); }
+extern "C" uint32_t td_emu_budget(uint32_t base, int a) { return td_attempt_budget(base, a); }
+extern "C" int td_emu_restarts(void) { return TD_RESTARTS; }
 bool tt_visit(uint64_t *tt, uint64_t L, int N, int lv, uint32_t gen) {
     const uint64_t data = N - 1 >= 16 ? ~0ull : ((1ull << (4 * (N - 1))) - 1ull);
     const uint64_t key = td_tt_key(L & data);

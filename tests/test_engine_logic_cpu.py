@@ -188,3 +188,21 @@ def test_restarts_keep_verdicts_and_witnesses(oracle, emu):
         emu.td_emu_set_restart(200)
     assert statuses[0] == statuses[16]
     assert 0 in statuses[0] and 1 in statuses[0]
+
+
+def test_restart_schedule(emu):
+    """The restart rule of td_core.cuh: Luby budgets, the first attempt in the
+    plain order, and the unbounded attempt after the budgeted ones in the
+    plain order too (the best single order for the long searches that get
+    that far); the attempts in between use distinct orders."""
+    R = emu.td_emu_restarts()
+    emu.td_emu_budget.restype = C.c_uint32
+    emu.td_emu_order.restype = C.c_uint32
+    luby = [1, 1, 2, 1, 1, 2, 4, 1, 1, 2, 1, 1, 2, 4, 8, 1]
+    assert [emu.td_emu_budget(16, a) for a in range(16)] == [16 * v for v in luby]
+    assert emu.td_emu_budget(16, R) == 0xFFFFFFFF and emu.td_emu_budget(0, 0) == 0xFFFFFFFF
+    for level in range(10):
+        assert emu.td_emu_order(0, level) == 0
+        assert emu.td_emu_order(R, level) == 0
+    first_orders = {emu.td_emu_order(a, 0) for a in range(R)}
+    assert len(first_orders) == R  # one order per budgeted attempt at the root
