@@ -123,6 +123,13 @@ def make_instances(td, rank, count=COUNT, workload="mix"):
     return td.prepare_perms(perms, n, MAX_MOVES), perms, n
 
 
+def bench_config(world: int, count: int = COUNT) -> dict:
+    """The workload definition both arms report (identical dicts)."""
+    return {"workload": WORKLOAD, "count_per_gpu": count, "seed": SEED, "max_moves": MAX_MOVES,
+            "l2": "GPU arm: inputs and scratch rewritten, L2 flushed between steps (256 MiB write)",
+            "parallelism": f"replicas x{world}"}
+
+
 def cpu_model() -> str:
     try:
         with open("/proc/cpuinfo") as f:
@@ -134,60 +141,164 @@ def cpu_model() -> str:
     return "unknown"
 
 
-def cpu_baseline(seconds_target=15.0, sample=96):
-    """The oracle (CPU restatement of the reference search, its single-queue
-    order) on all host cores, on a bounded sample of the workload."""
-    from oracle import oracle as O
-    import td16_b200 as td
-    perms, n = td.synth_perms(SEED, sample, 16, 16, 50, 1, 4)
-    c = len(n)
-    beta = np.zeros((c, 17), np.uint8)
-    omega = np.zeros((c, 17), np.uint8)
-    init = np.zeros(c, np.int32)
-    for i in range(c):
-        b, o, e = O.perm_to_pair(perms[i, :16].tolist())
+def _oracle_pairs(O, first, count):
+    """Instances [first, first + count) of the workload as reference pairs,
+    generated by the oracle's restatement of the seeded generator (the engine
+    library is not loaded)."""
+    perms, _ = O.synth_perms(SEED, first + count, 16, 16, 50, 1, 4)
+    beta = np.zeros((count, 17), np.uint8)
+    omega = np.zeros((count, 17), np.uint8)
+    init = np.zeros(count, np.int32)
+    for i in range(count):
+        b, o, e = O.perm_to_pair(perms[first + i, :16].tolist())
         beta[i], omega[i], init[i] = b, o, e
+    return beta, omega, init
+
+
+def cpu_reference_order(first=0, sample=96):
+    """The oracle -- the CPU restatement of the reference search in its
+    single-queue order -- on all host cores, on instances [first, first +
+    sample) of the workload.  Every witness is replayed by the oracle's
+    checker before it counts."""
+    from oracle import oracle as O
+    beta, omega, init = _oracle_pairs(O, first, sample)
     cores = os.cpu_count() or 1
     t0 = time.perf_counter()
-    st, dep, mv, ex = O.search_batch(beta, omega, np.full(c, 17), init, np.zeros(c), np.full(c, MAX_MOVES),
-                                     np.ones(c), cores)
+    st, dep, mv, ex = O.search_batch(beta, omega, np.full(sample, 17), init, np.zeros(sample),
+                                     np.full(sample, MAX_MOVES), np.ones(sample), cores)
     dt = time.perf_counter() - t0
-    # every oracle witness is replayed by the oracle's checker before it counts
     verified = 0
     for i in np.nonzero(st == 1)[0]:
         moves = [(int(m) & 31, (int(m) >> 5) & 31, (int(m) >> 10) & 31) for m in mv[i][: dep[i]]]
         abc = O.positions_to_symbols(beta[i].tolist(), moves)
         verified += O.validate(beta[i].tolist(), omega[i].tolist(), abc, MAX_MOVES) is None
     return {"value": verified / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"first {c} instances of the workload (seed {SEED}), {dt:.1f} s on {cores} threads",
-            "label": "CPU restatement of the reference algorithm (the reference has no CPU search)",
-            "nproc": os.cpu_count(), "cpu_model": cpu_model(),
-            "expansions_per_s": float(ex.sum()) / dt, "seconds": dt}
+            "sample": f"instances {first}..{first + sample - 1} of the workload (seed {SEED}), {dt:.1f} s on "
+                      f"{cores} threads",
+            "label": "CPU restatement of the reference algorithm, its single-queue order (the reference has "
+                     "no CPU search)",
+            "nproc": os.cpu_count(), "cpu_model": cpu_model(), "nodes_per_s": float(ex.sum()) / dt,
+            "expansions_per_witness": float(ex.sum()) / max(1, int((st == 1).sum())), "seconds": dt}
+
+
+def cpu_free_order(sample=16384):
+    """The engine's own free-order algorithm (restarts and explored-state
+    table; oracle/td_emu.cc, one lane at a time on the host) on all host
+    cores: the CPU figure for the same algorithm as the GPU arm."""
+    from oracle import oracle as O
+    beta, omega, init = _oracle_pairs(O, 0, sample)
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    res = O.emu_search_batch(beta, omega, 17, init, 0.0, MAX_MOVES, 1, 0, cores)
+    dt = time.perf_counter() - t0
+    found = int((res["status"] == 1).sum())
+    exp = float(res["expansions"].astype(np.int64).sum())
+    return {"searches_per_s": sample / dt, "witnesses_per_s": found / dt, "nodes_per_s": exp / dt,
+            "expansions_per_witness": exp / max(1, found), "cores": cores,
+            "sample": f"first {sample} instances of the workload, {dt:.1f} s on {cores} threads",
+            "label": "the engine's free-order algorithm emulated lane by lane on the host (test "
+                     "infrastructure, not tuned CPU code)"}
+
+
+def cpu_baseline():
+    base = cpu_reference_order()
+    base["free_order"] = cpu_free_order()
+    return base
 
 
 def run_reference(args):
+    """The reference arm: the CPU restatement of the reference search on the
+    host cores, each step a bounded consecutive sample of the same workload.
+    Loads the oracle only (no engine library)."""
     rank, world, _ = rank_info()
     if rank != 0:
         return
-    steps = []
-    for _ in range(args.warmup):
-        cpu_baseline(sample=16)
-    res = None
-    for _ in range(args.steps):
-        res = cpu_baseline(sample=48)
-        steps.append(res)
-    value = float(np.mean([s["value"] for s in steps]))
+    per_step = 48
+    for k in range(args.warmup):
+        cpu_reference_order(first=per_step * k, sample=16)
+    steps = [cpu_reference_order(first=per_step * k, sample=per_step) for k in range(args.steps)]
+    secs = float(np.sum([s["seconds"] for s in steps]))
+    verified = float(np.sum([s["value"] * s["seconds"] for s in steps]))
+    value = verified / secs
+    res = steps[-1]
+    cpu = {"value": value, "unit": UNIT, "cores": res["cores"], "kind": "port",
+           "sample": f"{args.steps} steps of {per_step} consecutive instances (instances 0.."
+                     f"{per_step * args.steps - 1} of the 2^20-instance workload), {secs:.1f} s on "
+                     f"{res['cores']} threads",
+           "label": res["label"], "nproc": res["nproc"], "cpu_model": res["cpu_model"],
+           "nodes_per_s": float(np.mean([s["nodes_per_s"] for s in steps]))}
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": float(np.mean([s["seconds"] for s in steps]) * 1e3),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/u64 integer",
-            "data": "synthetic (seeded)", "config": {"workload": WORKLOAD, "count": COUNT, "seed": SEED,
-                                                     "max_moves": MAX_MOVES, "l2": "n/a (CPU)"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": res["cores"], "kind": "port",
-                             "sample": res["sample"], "label": res["label"], "nproc": res["nproc"],
-                             "cpu_model": res["cpu_model"]},
+            "data": "synthetic (seeded)", "config": bench_config(args.gpus),
+            "nodes_per_s": cpu["nodes_per_s"], "cpu_baseline": cpu,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libtd16ref.so")
+
+
+def per_call_legs(td, k=8192, slots=16, budget=1 << 30):
+    """One blocking search per call from `slots` native threads, one per slot,
+    as the emitter's Java slot workers call searchForSortingSeq: this engine's
+    td_search, and the reference kernel itself (sorting_search.cu and
+    slot_manager.cu compiled unmodified for sm_100a into oracle/_ref, when that
+    build exists) on the same first k instances of the workload."""
+    from td16_b200 import _lib
+    perms, n = td.synth_perms(SEED, k, 16, 16, 50, 1, 4)
+    beta = np.zeros((k, 17), np.uint8)
+    omega = np.zeros((k, 17), np.uint8)
+    init = np.zeros(k, np.int32)
+    pairs_b = np.zeros(17, np.uint8)
+    pairs_o = np.zeros(17, np.uint8)
+    td_lib = _lib.lib()
+    for i in range(k):
+        td_lib.td_pairs_from_perms(1, perms[i:].ctypes.data, n[i:].ctypes.data, pairs_b.ctypes.data,
+                                   pairs_o.ctypes.data)
+        beta[i], omega[i] = pairs_b, pairs_o
+    inst = td.prepare_perms(perms, n, MAX_MOVES)
+    init[:] = inst["packed"] & 31
+    out = {"workload": f"first {k} instances of the benchmark workload, bound {MAX_MOVES}, one blocking "
+                       f"search per call from {slots} native threads (one per slot)"}
+    td.init_slots(slots, [0], budget)
+    try:
+        fn = _lib.entry_address("td_search")
+        _lib.slot_threads_run(fn, beta[:512], omega[:512], 17, init[:512], 0.0, MAX_MOVES, 1, slots)  # warm-up
+        r = _lib.slot_threads_run(fn, beta, omega, 17, init, 0.0, MAX_MOVES, 1, slots)
+        lat = np.sort(r["latency_s"]) * 1e3
+        out["engine_td_search"] = {"per_s": k / r["seconds"], "seconds": r["seconds"],
+                                   "found": int((r["status"] == 1).sum()), "errors": int((r["status"] < 0).sum()),
+                                   "p50_ms": float(lat[k // 2]), "p99_ms": float(lat[int(0.99 * (k - 1))])}
+        engine_status = r["status"]
+    finally:
+        td.destroy()
+    if not os.path.exists(REF_LIB):
+        out["reference_kernel"] = {"unavailable": "oracle/_ref/libtd16ref.so was not built (needs the reference "
+                                                  "checkout at build time)"}
+        return out
+    import ctypes as C
+    ref = C.CDLL(REF_LIB)
+    ref.ref_init.argtypes = [C.c_int, C.c_int, C.c_ulonglong, C.c_char_p, C.c_size_t]
+    err = C.create_string_buffer(512)
+    if ref.ref_init(slots, 0, budget, err, 512) != 0:
+        out["reference_kernel"] = {"unavailable": err.value.decode()}
+        return out
+    try:
+        fn = C.cast(ref.ref_search, C.c_void_p).value
+        _lib.slot_threads_run(fn, beta[:512], omega[:512], 17, init[:512], 0.0, MAX_MOVES, 1, slots, kind=1)
+        r = _lib.slot_threads_run(fn, beta, omega, 17, init, 0.0, MAX_MOVES, 1, slots, kind=1)
+    finally:
+        ref.ref_destroy()
+    lat = np.sort(r["latency_s"]) * 1e3
+    out["reference_kernel"] = {"per_s": k / r["seconds"], "seconds": r["seconds"],
+                               "found": int((r["status"] == 1).sum()), "errors": int((r["status"] < 0).sum()),
+                               "p50_ms": float(lat[k // 2]), "p99_ms": float(lat[int(0.99 * (k - 1))]),
+                               "source": "sorting_search.cu + slot_manager.cu, unmodified, sm_100a"}
+    both = (engine_status >= 0) & (r["status"] >= 0)
+    out["verdicts_agree"] = bool((engine_status[both] == r["status"][both]).all())
+    out["engine_over_reference"] = out["engine_td_search"]["per_s"] / out["reference_kernel"]["per_s"]
+    return out
 
 
 def run_engine(args):
@@ -270,12 +381,17 @@ def run_engine(args):
     e2e_s, e2e_verified = 0.0, 0
     if not only_engine:
         td.search_batch(0, host_in, _lib.FLAG_VERIFY, out=host_out)  # untimed: sizes the slot's batch buffer
-    for k in range(0 if only_engine else max(1, min(args.steps, 3))):
+    e2e_ms = []
+    for k in range(0 if only_engine else args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        torch.cuda.synchronize()
         t0 = time.perf_counter()
         res_h, st = td.search_batch(0, host_in, _lib.FLAG_VERIFY, out=host_out)
-        e2e_s += time.perf_counter() - t0
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
         e2e_verified += int((res_h["status"] == 1).sum())
-    e2e_steps = max(1, min(args.steps, 3))
+    e2e_s = sum(e2e_ms) / 1e3
+    e2e_steps = max(1, len(e2e_ms))
 
     # the plain one-launch-per-batch form on the same GPU
     plain_ms, plain_verified = float("nan"), 0
@@ -304,6 +420,9 @@ def run_engine(args):
     _lib.check(_lib.lib().td_int_issue_peak(local, 200.0, C.byref(issue_peak), C.byref(alu_peak), err, 256), err)
     per_step_exp = expansions / max(1, args.steps) / world
     mean_ms = float(np.mean(step_ms))
+    clock = clocks.summary()
+    sm_mhz = clock["sm_mhz"] or 1965.0
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
     nodes_per_s = per_step_exp / (mean_ms / 1e3)
     triples_per_s = nodes_per_s * 680
     # The bound is the integer ALU pipe (LOP3/shift/compare work of the
@@ -316,7 +435,11 @@ def run_engine(args):
                 "peak_source": "measured live: LOP3 chains on every SM (td_int_issue_peak), of measured",
                 "alu_inst_per_expansion": ALU_INST_PER_EXPANSION,
                 "issue_achieved": nodes_per_s * INST_PER_EXPANSION / 1e9,
-                "issue_peak_lop3_imad": issue_peak.value / 1e9,
+                # issue: 4 warp instructions per clock per SM (one per
+                # sub-partition) at the SM clock sampled during the timed steps
+                "issue_peak_4_per_clk": 4 * sms * sm_mhz * 1e6 / 1e9,
+                "issue_frac": nodes_per_s * INST_PER_EXPANSION / (4 * sms * sm_mhz * 1e6),
+                "issue_lop3_imad_measured": issue_peak.value / 1e9,
                 "inst_per_expansion": INST_PER_EXPANSION,
                 "traffic": DRAM_BYTES_PER_2P18_LAUNCH * count / (1 << 18),
                 "traffic_note": "DRAM bytes per launch: ncu on the first 2^18 instances, scaled by instance count "
@@ -339,22 +462,24 @@ def run_engine(args):
         _, bst = td.search_batch(0, inst_s, 0)
         serving["batched_per_s"] = len(inst_s) / (bst.kernel_ms / 1e3)
     cpu = cpu_baseline() if world == 1 and not only_engine else None
+    percall = per_call_legs(td) if world == 1 and not only_engine else None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": mean_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8/u64 integer", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD, "count_per_gpu": count, "seed": SEED, "max_moves": MAX_MOVES,
-                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
+        "config": bench_config(world, count),
         "nodes_per_s": nodes_per_s, "triples_per_s": triples_per_s,
         "found": found, "not_found": not_found, "errors": errors, "verified": verified,
         "plain_one_launch": {"value": plain_verified / (plain_ms / 1e3), "ms": plain_ms},
         "e2e": {"value": e2e_verified / e2e_s if e2e_s else None, "unit": UNIT, "h2d_bytes_per_step": count * 16,
-                "d2h_bytes_per_step": count * 32, "ms_per_step": e2e_s / e2e_steps * 1e3},
-        "gpu_launches": args.steps * 3,
+                "d2h_bytes_per_step": count * 32, "ms_per_step": e2e_s / e2e_steps * 1e3, "steps": len(e2e_ms),
+                "ms_min": min(e2e_ms) if e2e_ms else None, "ms_max": max(e2e_ms) if e2e_ms else None},
+        "gpu_launches": args.steps * 4,  # per graph replay: epoch, search, finalize, replay
         "launch_shape": tuned,
         "roofline": roofline,
-        "clocks": clocks.summary(),
+        "clocks": clock,
         "cpu_baseline": cpu,
+        "percall": percall,
         "serving": serving,
     }
     print(json.dumps(line), flush=True)

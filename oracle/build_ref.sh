@@ -1,8 +1,9 @@
 #!/usr/bin/env bash
 # Builds oracle/_ref/libtd16ref.so from the reference's own native sources
 # (read in place, unmodified) plus oracle/ref_driver.cu.  TEST INFRASTRUCTURE
-# ONLY.  Needs the reference checkout; on machines without it the prebuilt
-# library (if any) is used as is.
+# ONLY.  The reference checkout is taken from TD16_REFERENCE (this recipe's
+# default is the build container's read-only checkout); where it is absent the
+# recipe skips, and the prebuilt library (if any) is used as is.
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
 REF="${TD16_REFERENCE:-/root/reference}/emitter/src/native"

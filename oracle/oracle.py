@@ -19,6 +19,7 @@ MAX_N = 17
 MAX_DEPTH = 9
 FOUND = 1
 NOT_FOUND = 0
+BUDGET = -2
 
 _lib = None
 
@@ -56,6 +57,10 @@ def lib():
         L.tdo_apply_transposition.argtypes = [u8p, C.c_int, C.c_int, C.c_int, C.c_int, u8p]
         L.tdo_compose.argtypes = [u8p, u8p, C.c_int, u8p]
         L.tdo_cycle_oneline.argtypes = [u8p, C.c_int, C.c_int, u8p]
+        L.tdo_set_expansion_budget.argtypes = [C.c_uint64]
+        L.tdo_set_expansion_budget.restype = None
+        L.tdo_synth_perms.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                      C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -89,6 +94,11 @@ def accepts(n, init_odd, min_rate, full, odd, depth) -> bool:
 
 def can_reach(n, init_odd, min_rate, max_depth, full, odd, depth) -> bool:
     return bool(lib().tdo_can_reach(n, init_odd, min_rate, max_depth, int(full), odd, depth))
+
+
+def set_expansion_budget(max_expansions: int) -> None:
+    """Later searches give up (status BUDGET) after this many expansions; 0 = never."""
+    lib().tdo_set_expansion_budget(int(max_expansions))
 
 
 def search(beta, omega, init_odd, min_rate, max_moves, full=True):
@@ -128,6 +138,17 @@ def search_batch(beta, omega, n, init_odd, min_rate, max_depth, full, threads=1)
     if rc != 0:
         raise ValueError("tdo_search_batch rejected its arguments")
     return status, depth, moves, exp
+
+
+def synth_perms(seed: int, count: int, n_min: int, n_max: int, hard_pct: int, hard_min: int, hard_max: int):
+    """The benchmark's seeded S_n instances: (perms int8[count, 16], n uint8[count])."""
+    perms = np.zeros((count, 16), np.int8)
+    n = np.zeros(count, np.uint8)
+    rc = lib().tdo_synth_perms(C.c_uint64(seed), int(count), n_min, n_max, hard_pct, hard_min, hard_max,
+                               perms.ctypes.data_as(C.c_void_p), n.ctypes.data_as(C.c_void_p))
+    if rc != 0:
+        raise ValueError("invalid synthetic-instance parameters")
+    return perms, n
 
 
 def perm_to_pair(pi):
@@ -209,3 +230,52 @@ def cycle_oneline(cyc, n):
     out = (C.c_uint8 * max(1, n))()
     lib().tdo_cycle_oneline(_u8(cyc), len(cyc), n, out)
     return list(out[:n])
+
+
+# ---- host emulation of the engine's algorithm (libtdemu.so) -----------------
+#
+# Not a parity oracle: td_emu.cc restates the engine's own warp algorithm one
+# lane at a time.  The CPU tests use it to check the engine's logic, and the
+# benchmark's CPU baseline times the free-order algorithm with it.
+
+EMU_PATH = os.path.join(HERE, "libtdemu.so")
+EMU_INSTANCE = np.dtype([("perm", "<u8"), ("min_rate", "<f4"), ("n_symbols", "u1"), ("offset", "u1"),
+                         ("max_moves", "u1"), ("packed", "u1")])
+EMU_RESULT = np.dtype([("status", "<i4"), ("depth", "<i4"), ("moves", "<u2", (9,)), ("reserved", "<u2"),
+                       ("expansions", "<u4")])
+_emu = None
+
+
+def emu():
+    global _emu
+    if _emu is None:
+        if not os.path.exists(EMU_PATH):
+            build()
+        E = C.CDLL(EMU_PATH)
+        E.td_emu_prepare_pair.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int, C.c_int,
+                                          C.c_void_p]
+        E.td_emu_search_batch.argtypes = [C.c_int, C.c_void_p, C.c_uint, C.c_void_p, C.c_int]
+        _emu = E
+    return _emu
+
+
+def emu_search_batch(beta, omega, n, init_odd, min_rate, max_depth, full, flags=0, threads=1):
+    """The engine's algorithm on host threads (flags 0: free order with its
+    restarts and explored-state table; 1: reference order).  Arrays as for
+    search_batch.  Returns an EMU_RESULT array."""
+    count = int(beta.shape[0])
+    beta = np.ascontiguousarray(beta, np.uint8)
+    omega = np.ascontiguousarray(omega, np.uint8)
+    bc = lambda v, dt: np.broadcast_to(np.asarray(v, dt), (count,))  # noqa: E731
+    n, init_odd, min_rate = bc(n, np.int32), bc(init_odd, np.int32), bc(min_rate, np.float32)
+    max_depth, full = bc(max_depth, np.int32), bc(full, np.int32)
+    inst = np.zeros(count, EMU_INSTANCE)
+    E = emu()
+    for i in range(count):
+        if E.td_emu_prepare_pair(beta[i].ctypes.data, omega[i].ctypes.data, int(n[i]), int(init_odd[i]),
+                                 float(min_rate[i]), int(max_depth[i]), int(full[i]),
+                                 inst[i:].ctypes.data) != 0:
+            raise ValueError(f"instance {i} is not a valid pair")
+    res = np.zeros(count, EMU_RESULT)
+    E.td_emu_search_batch(count, inst.ctypes.data, int(flags), res.ctypes.data, int(threads))
+    return res

@@ -1,8 +1,11 @@
 // td_emu.cc -- serial host emulation of the engine's warp algorithm.
 //
-// TEST INFRASTRUCTURE ONLY.  It runs the kernel's per-node steps one lane at a
-// time, so the CPU test suite can check the engine's logic against the oracle
-// without a GPU:
+// TEST INFRASTRUCTURE ONLY, and not a parity oracle: it restates the engine's
+// own algorithm, not the reference's.  It runs the kernel's per-node steps one
+// lane at a time, so that the CPU test suite can check the engine's logic
+// against the oracle (td_oracle.c) without a GPU, and so that the benchmark's
+// CPU baseline can time the free-order algorithm on host cores
+// (td_emu_search_batch):
 //   reference order: pinned state, pair table, 12-bit class table, per-lane
 //     step bitmasks and the single-queue child order;
 //   free order: row masks and bit-sliced classes (td_row_classes), pair slots,
@@ -10,9 +13,13 @@
 //     with their child orders (td_attempt_budget, td_level_order).
 // It shares the kernel's helpers in td_core.cuh.  The product library does not
 // contain or call it.
-#include "../../td16_b200/csrc/td_core.cuh"
+#include "../td16_b200/csrc/td_core.cuh"
 
 #include <string.h>
+
+#include <atomic>
+#include <thread>
+#include <vector>
 
 namespace {
 
@@ -438,4 +445,19 @@ extern "C" int td_emu_prepare_pair(const uint8_t *beta, const uint8_t *omega, in
 
 extern "C" void td_emu_apply_move(uint64_t L, int off, int N, int i, int j, int k, uint64_t *outL, int *outOff) {
     td_apply_move(L, off, N, i, j, k, outL, outOff);
+}
+
+// `count` independent searches on `threads` host threads, one instance per
+// thread at a time (the CPU baseline of the free order).  flags as for
+// td_emu_search.  Returns 0.
+extern "C" int td_emu_search_batch(int count, const td_instance *x, unsigned flags, td_result *res, int threads) {
+    std::atomic<int> next{0};
+    auto work = [&] {
+        for (int i = next.fetch_add(1); i < count; i = next.fetch_add(1)) td_emu_search(&x[i], flags, &res[i]);
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < threads; ++t) pool.emplace_back(work);
+    work();
+    for (auto &t : pool) t.join();
+    return 0;
 }

@@ -171,9 +171,15 @@ static int make_child(const tdo_node *parent, int n, int i, int j, int k,
     return 1;
 }
 
+/* Expansion budget of later searches (0 = none): lets fixture generators
+ * drop candidate cases whose trees are too large to search in a test. */
+static _Atomic uint64_t g_budget = 0;
+void tdo_set_expansion_budget(uint64_t max_expansions) { atomic_store(&g_budget, max_expansions); }
+
 int tdo_search(const uint8_t *beta, const uint8_t *omega, int n, int init_odd,
                float min_rate, int max_depth, int full, uint16_t *out_moves,
                int *out_depth, tdo_stats *stats) {
+    const uint64_t budget = atomic_load(&g_budget);
     if (out_depth) *out_depth = 0;
     if (n < 0 || n > TDO_MAX_N) return TDO_EINVAL;
     if (max_depth <= 0 || max_depth > TDO_MAX_DEPTH) return TDO_EINVAL;
@@ -229,6 +235,10 @@ int tdo_search(const uint8_t *beta, const uint8_t *omega, int n, int init_odd,
         if (node.depth >= max_depth ||
             !tdo_can_reach(n, init_odd, min_rate, max_depth, full, node.odd, node.depth))
             continue;
+        if (budget && local.expansions >= budget) {
+            status = TDO_BUDGET;
+            goto done;
+        }
         local.expansions++;
         const int child_depth = node.depth + 1;
 
@@ -536,4 +546,103 @@ int tdo_codec_decode_value(const uint8_t *in, int len, uint8_t *abc, int cap) {
     if (cap < count) return -1;
     for (int m = 0; m < 3 * count; ++m) abc[m] = (uint8_t)get_symbol(in, 5 * m);
     return count;
+}
+
+/* ---- seeded synthetic instances ------------------------------------------
+ *
+ * The benchmark's instance generator, restated here so that the CPU baseline
+ * and the reference arm of bench.py build their inputs without loading the
+ * engine library.  A CPU test checks it bit for bit against the engine's
+ * td_synth_perms.  Published methods only:
+ *   - splitmix64 (Steele, Lea, Flood, "Fast splittable pseudorandom number
+ *     generators", OOPSLA 2014), one stream per instance seeded seed ^ index;
+ *   - Lemire's multiply-shift bounded integer with rejection ("Fast random
+ *     integer generation in an interval", TOMACS 2019) on the top 32 bits of
+ *     each draw;
+ *   - Fisher-Yates from the last position down for the uniform permutations;
+ *   - for the hard ones, the reverse permutation composed with a uniform
+ *     number of block transpositions, each a uniform lexicographic rank over
+ *     the triples x < y < z of {0..n} (blocks [x,y) and [y,z) swapped). */
+
+static uint64_t synth_next(uint64_t *state) {
+    *state += 0x9E3779B97F4A7C15ull;
+    uint64_t z = *state;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+static uint32_t synth_below(uint64_t *state, uint32_t bound) {
+    uint64_t product = (uint64_t)(uint32_t)(synth_next(state) >> 32) * bound;
+    if ((uint32_t)product < bound) {
+        const uint32_t floor_rem = (uint32_t)(-bound) % bound;
+        while ((uint32_t)product < floor_rem)
+            product = (uint64_t)(uint32_t)(synth_next(state) >> 32) * bound;
+    }
+    return (uint32_t)(product >> 32);
+}
+
+/* rank -> (x, y, z), lexicographic over x < y < z <= n */
+static void synth_triple(int n, uint32_t rank, int *x, int *y, int *z) {
+    for (int a = 0; a <= n - 2; ++a) {
+        const int rest = n - a;  /* symbols after a */
+        const uint32_t with_a = (uint32_t)(rest * (rest - 1) / 2);
+        if (rank >= with_a) {
+            rank -= with_a;
+            continue;
+        }
+        for (int b = a + 1; b <= n - 1; ++b) {
+            const uint32_t with_b = (uint32_t)(n - b);
+            if (rank < with_b) {
+                *x = a;
+                *y = b;
+                *z = b + 1 + (int)rank;
+                return;
+            }
+            rank -= with_b;
+        }
+    }
+    *x = 0;
+    *y = 1;
+    *z = 2;
+}
+
+int tdo_synth_perms(uint64_t seed, int count, int n_min, int n_max, int hard_pct,
+                    int hard_min, int hard_max, int8_t *perms, uint8_t *n_out) {
+    if (count < 0 || n_min < 1 || n_max > 16 || n_min > n_max || hard_min < 0 ||
+        hard_max < hard_min)
+        return TDO_EINVAL;
+    for (int idx = 0; idx < count; ++idx) {
+        uint64_t state = seed ^ (uint64_t)idx;
+        const int n = n_min + (int)synth_below(&state, (uint32_t)(n_max - n_min + 1));
+        int8_t *p = perms + (size_t)idx * 16;
+        const int hard = (int)synth_below(&state, 100) < hard_pct;
+        if (hard) {
+            for (int m = 0; m < n; ++m) p[m] = (int8_t)(n - 1 - m);
+            const int moves = hard_min + (int)synth_below(&state, (uint32_t)(hard_max - hard_min + 1));
+            const uint32_t ranks = (uint32_t)((n + 1) * n * (n - 1) / 6);
+            for (int mv = 0; mv < moves && ranks > 0; ++mv) {
+                int x, y, z;
+                synth_triple(n, synth_below(&state, ranks), &x, &y, &z);
+                int8_t swapped[16];
+                int w = 0;
+                for (int q = 0; q < x; ++q) swapped[w++] = p[q];
+                for (int q = y; q < z; ++q) swapped[w++] = p[q];
+                for (int q = x; q < y; ++q) swapped[w++] = p[q];
+                for (int q = z; q < n; ++q) swapped[w++] = p[q];
+                memcpy(p, swapped, (size_t)n);
+            }
+        } else {
+            for (int m = 0; m < n; ++m) p[m] = (int8_t)m;
+            for (int m = n - 1; m > 0; --m) {
+                const int j = (int)synth_below(&state, (uint32_t)(m + 1));
+                const int8_t t = p[m];
+                p[m] = p[j];
+                p[j] = t;
+            }
+        }
+        for (int m = n; m < 16; ++m) p[m] = 0;
+        n_out[idx] = (uint8_t)n;
+    }
+    return 0;
 }

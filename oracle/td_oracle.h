@@ -30,6 +30,7 @@ extern "C" {
 #define TDO_NOT_FOUND 0
 #define TDO_FOUND 1
 #define TDO_EINVAL (-1)
+#define TDO_BUDGET (-2)  /* the expansion budget ran out before a verdict */
 
 typedef struct {
     uint64_t expansions; /* nodes whose children were evaluated */
@@ -62,6 +63,11 @@ int tdo_search(const uint8_t *beta, const uint8_t *omega, int n, int init_odd,
                float min_rate, int max_depth, int full,
                uint16_t *out_moves, int *out_depth, tdo_stats *stats);
 
+/* Expansion budget of every later search (0, the default, = none): a search
+ * that would expand more nodes returns TDO_BUDGET.  For screening candidate
+ * test cases only. */
+void tdo_set_expansion_budget(uint64_t max_expansions);
+
 /* Batch of independent searches on `threads` host threads (one instance per
  * thread at a time).  Records are laid out with strides of TDO_MAX_N bytes
  * (beta, omega) and TDO_MAX_DEPTH moves.  Returns 0 or TDO_EINVAL. */
@@ -75,6 +81,15 @@ int tdo_search_batch(int count, const uint8_t *beta, const uint8_t *omega,
 /* S_n instance (pi over 0..n-1) -> reference pair over N = n+1 symbols */
 void tdo_perm_to_pair(const int8_t *pi, int n, uint8_t *beta, uint8_t *omega,
                       int *init_odd);
+
+/* The benchmark's seeded instances (int8 stride 16), generated without the
+ * engine library: instance i draws from splitmix64 seeded seed ^ i; n
+ * uniform in [n_min, n_max]; with probability hard_pct/100 the reverse
+ * permutation composed with hard_min..hard_max uniform block transpositions,
+ * else a Fisher-Yates uniform permutation.  Same output as the engine's
+ * td_synth_perms. */
+int tdo_synth_perms(uint64_t seed, int count, int n_min, int n_max, int hard_pct,
+                    int hard_min, int hard_max, int8_t *perms, uint8_t *n_out);
 
 /* position triples -> symbol triples, evolving a copy of beta
  * (GPUSortingSearch.java:229-238) */

@@ -422,3 +422,52 @@ class BatchGraph:
         if self._h:
             lib().td_batch_graph_destroy(self._h)
             self._h = None
+
+
+# ---- native slot threads (td_slot_threads.cc) ---------------------------------
+
+THREADS_PATH = os.path.join(PKG, "libtd16_slot_threads.so")
+_threads = None
+
+
+def _threads_lib():
+    global _threads
+    if _threads is None:
+        if not os.path.exists(THREADS_PATH):
+            raise ImportError(f"{THREADS_PATH} is missing: build it with `python -m td16_b200.build`")
+        h = C.CDLL(THREADS_PATH)
+        h.td_slot_threads_run.restype = C.c_double
+        h.td_slot_threads_run.argtypes = [C.c_int, C.c_void_p, C.c_int] + [C.c_void_p] * 7 + [
+            C.c_int, C.c_int] + [C.c_void_p] * 5
+        _threads = h
+    return _threads
+
+
+def slot_threads_run(fn, beta, omega, n, init, rate, maxd, full, threads: int, first_slot: int = 0,
+                     kind: int = 0):
+    """Runs one blocking search per instance from `threads` native threads
+    (thread t on slot first_slot + t), through the entry point at address
+    `fn` (kind 0: td_search's signature; kind 1: the reference driver's).
+    beta/omega uint8[count, 17]; the rest per instance.  Returns a dict with
+    the wall time, status (1 found, 0 not found, -1 error), the entry's return
+    codes, depths, position moves int16[count, 9, 3] and per-call latencies."""
+    count = int(beta.shape[0])
+    beta = np.ascontiguousarray(beta, np.uint8)
+    omega = np.ascontiguousarray(omega, np.uint8)
+    bc = lambda v, dt: np.ascontiguousarray(np.broadcast_to(v, (count,)), dt)  # noqa: E731
+    n, init, rate, maxd, full = (bc(n, np.int32), bc(init, np.int32), bc(rate, np.float32), bc(maxd, np.int32),
+                                 bc(full, np.uint8))
+    status = np.zeros(count, np.int32)
+    code = np.zeros(count, np.int32)
+    depth = np.zeros(count, np.int32)
+    moves = np.zeros((count, 9, 3), np.int16)
+    lat = np.zeros(count, np.float64)
+    secs = _threads_lib().td_slot_threads_run(int(kind), C.c_void_p(fn), count, *[_ptr(a) for a in (
+        beta, omega, n, init, rate, maxd, full)], int(threads), int(first_slot),
+        *[_ptr(a) for a in (status, code, depth, moves, lat)])
+    return {"seconds": secs, "status": status, "code": code, "depth": depth, "moves": moves, "latency_s": lat}
+
+
+def entry_address(name: str) -> int:
+    """Address of an entry point of the engine library (for slot_threads_run)."""
+    return C.cast(getattr(lib(), name), C.c_void_p).value

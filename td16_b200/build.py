@@ -12,6 +12,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libtd16b200.so")
 JNI_LIB = os.path.join(PKG, "libtd16_jni.so")
+THREADS_LIB = os.path.join(PKG, "libtd16_slot_threads.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hidden",
@@ -30,14 +31,15 @@ def _sources():
 
 
 def _deps():
-    return glob.glob(os.path.join(CSRC, "*")) + [os.path.join(PKG, "..", "include", "td16_b200.h")]
+    return [p for p in glob.glob(os.path.join(CSRC, "*")) if p.endswith((".cu", ".cuh"))] + [
+        os.path.join(PKG, "..", "include", "td16_b200.h")]
 
 
-def up_to_date(target: str) -> bool:
+def up_to_date(target: str, deps=None) -> bool:
     if not os.path.exists(target):
         return False
     t = os.path.getmtime(target)
-    return all(os.path.getmtime(d) <= t for d in _deps() if os.path.exists(d))
+    return all(os.path.getmtime(d) <= t for d in (deps if deps is not None else _deps()) if os.path.exists(d))
 
 
 def build(verbose: bool = False, force: bool = False) -> str:
@@ -50,8 +52,22 @@ def build(verbose: bool = False, force: bool = False) -> str:
             sys.stderr.write(res.stdout + res.stderr)
         if res.returncode != 0:
             raise RuntimeError("nvcc failed building libtd16b200.so")
+    _build_slot_threads(verbose, force)
     _build_jni(verbose)
     return LIB
+
+
+def _build_slot_threads(verbose: bool, force: bool) -> None:
+    """Native slot threads that drive a blocking search entry (td_slot_threads.cc)."""
+    src = os.path.join(CSRC, "td_slot_threads.cc")
+    if not force and up_to_date(THREADS_LIB, [src]):
+        return
+    cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-pthread", "-fvisibility=hidden", "-o", THREADS_LIB, src]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if verbose or res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+    if res.returncode != 0:
+        raise RuntimeError("g++ failed building libtd16_slot_threads.so")
 
 
 def _jni_include():

@@ -345,6 +345,29 @@ __global__ void td_epoch_kernel(uint32_t *epoch) {
     *epoch = e ? e : 1;
 }
 
+// Runs after td_steal_kernel on the same stream.  When a bounded wait of the
+// launch gave up (pool->error), some instances may have no result record: one
+// never claimed, or one whose donated subtree a taker never received (its
+// pending count stays above zero, so no unit wrote the final status).  Those
+// get a timeout record, so a caller never reads a stale record of an earlier
+// launch.  Without an error every thread returns at once.
+__global__ void __launch_bounds__(256) td_finalize_kernel(const td_pool *__restrict__ pool,
+                                                          const td_inst_state *__restrict__ state,
+                                                          td_result *__restrict__ out, int count) {
+    if (*(volatile const int *)&pool->error == 0) return;
+    const int claimed = min(count, *(volatile const int *)&pool->inst_ticket);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        if (i < claimed && state[i].pending == 0) continue;
+        td_result r;
+        r.status = TD_ERR_TIMEOUT;
+        r.depth = 0;
+        for (int m = 0; m < TD_MAX_DEPTH; ++m) r.moves[m] = 0;
+        r.reserved = 0;
+        r.expansions = i < claimed ? state[i].expansions : 0;
+        out[i] = r;
+    }
+}
+
 // The totals of td_batch_stats, reduced on the device so that the host does
 // not walk the result array (2^20 results are 32 MiB of host memory).  Reads
 // only the status and expansion words of each record.
@@ -537,6 +560,49 @@ uint64_t time_limit_ns() {
     return v;
 }
 
+// The launch settings of one launch, read together under g_mu so that a
+// concurrent td_configure_* call never hands a launch half of its change.
+struct LaunchCfg {
+    int warps, grain, steal_grain, split_level, check_every, tt_bits;
+    uint32_t restart_base;
+    int serve_grain, serve_split_level, serve_check_every;
+    int sms, steal_blocks_per_sm, blocks_per_sm;  // of the device, for `warps`
+};
+
+// Snapshot of the settings and of `device`'s occupancy for them; the device
+// must be current and set up (ensure_device).
+int launch_cfg(int device, LaunchCfg *c, char *err, size_t errlen) {
+    std::lock_guard<std::mutex> g(g_mu);
+    c->warps = g_warps_per_block;
+    c->grain = g_grain;
+    c->steal_grain = g_steal_grain;
+    c->split_level = g_split_level;
+    c->check_every = g_check_every;
+    c->tt_bits = g_tt_bits;
+    c->restart_base = g_restart_base;
+    c->serve_grain = g_serve_grain;
+    c->serve_split_level = g_serve_split_level;
+    c->serve_check_every = g_serve_check_every;
+    DeviceInfo &d = g_dev[device];
+    const int threads = c->warps * 32;
+    if (d.steal_blocks_per_sm == 0) {
+        int b = 0;
+        TD_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, td_steal_kernel, threads,
+                                                               steal_smem_bytes(c->warps)));
+        d.steal_blocks_per_sm = std::max(1, b);
+    }
+    if (d.blocks_per_sm == 0) {
+        int b = 0;
+        TD_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, td_persistent_kernel<false>, threads,
+                                                               smem_bytes(c->warps)));
+        d.blocks_per_sm = std::max(1, b);
+    }
+    c->sms = d.sms;
+    c->steal_blocks_per_sm = d.steal_blocks_per_sm;
+    c->blocks_per_sm = d.blocks_per_sm;
+    return TD_OK;
+}
+
 int ensure_device(int device, char *err, size_t errlen) {
     if ((int)g_dev.size() <= device) g_dev.resize(device + 1);
     DeviceInfo &d = g_dev[device];
@@ -600,7 +666,10 @@ int launch_batch(Slot &s, int count, const td_instance *d_in, td_result *d_out, 
                  uint64_t max_exp, cudaStream_t stream, char *err, size_t errlen) {
     if (count <= 0) return TD_OK;
     const bool ordered = flags & TD_FLAG_ORDERED;
-    const int warps = g_warps_per_block;
+    LaunchCfg cfg;
+    const int rc = launch_cfg(s.device, &cfg, err, errlen);
+    if (rc != TD_OK) return rc;
+    const int warps = cfg.warps;
     const size_t smem = smem_bytes(warps);
     const int threads = warps * 32;
     if (flags & TD_FLAG_PLAIN) {
@@ -627,52 +696,43 @@ int launch_batch(Slot &s, int count, const td_instance *d_in, td_result *d_out, 
             TD_CHECK(cudaMalloc(&s.d_state, (size_t)count * sizeof(td_inst_state)));
             s.state_count = (size_t)count;
         }
-        DeviceInfo &d = g_dev[s.device];
-        if (d.steal_blocks_per_sm == 0) {
-            int b = 0;
-            TD_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, td_steal_kernel, threads, steal_smem_bytes(warps)));
-            d.steal_blocks_per_sm = std::max(1, b);
-        }
         // at least the slot's share of the resident grid, so that a small batch
         // (one search from td_search) is spread over that many warps by donation
-        const int resident = d.sms * d.steal_blocks_per_sm;
+        const int resident = cfg.sms * cfg.steal_blocks_per_sm;
         const int share = std::max(1, resident / std::max(1, s.slots_on_device));
         const int grid = std::max(1, std::min(resident, std::max(share, (count + warps - 1) / warps)));
-        if (g_tt_bits > 0 && ((size_t)resident * warps > s.tt_warps || g_tt_bits != s.tt_bits)) {
-            // one table (8 bytes x 2^TD_TT_BITS) per resident warp, sized for
+        if (cfg.tt_bits > 0 && ((size_t)resident * warps > s.tt_warps || cfg.tt_bits != s.tt_bits)) {
+            // one table (8 bytes x 2^tt_bits) per resident warp, sized for
             // the whole resident grid so that it never moves under a captured
             // graph; the launch waits for the previous one before replacing it
             TD_CHECK(cudaStreamSynchronize(stream));
             if (s.d_tt) TD_CHECK(cudaFree(s.d_tt));
             s.d_tt = nullptr;
             s.tt_warps = 0;
-            TD_CHECK(cudaMalloc(&s.d_tt, ((size_t)resident * warps << g_tt_bits) * sizeof(uint64_t)));
+            TD_CHECK(cudaMalloc(&s.d_tt, ((size_t)resident * warps << cfg.tt_bits) * sizeof(uint64_t)));
             s.tt_warps = (size_t)resident * warps;
-            s.tt_bits = g_tt_bits;
+            s.tt_bits = cfg.tt_bits;
         }
         TD_CHECK(cudaMemsetAsync(s.d_pool, 0, sizeof(td_pool), stream));
         TD_CHECK(cudaMemsetAsync(s.d_state, 0, (size_t)count * sizeof(td_inst_state), stream));
         td_epoch_kernel<<<1, 1, 0, stream>>>(s.d_epoch);
-        td_steal_kernel<<<grid, threads, steal_smem_bytes(warps), stream>>>(d_in, d_out, count, s.d_pool, s.d_items,
-                                                                            s.d_ready, s.d_epoch,
-                                                         s.item_capacity, s.d_state, g_steal_grain, g_split_level,
-                                                         g_check_every, time_limit_ns(), g_tt_bits > 0 ? s.d_tt : nullptr,
-                                                         g_tt_bits, g_restart_base, max_exp,
-                                                         count == 1 ? 4096u : 32768u);
+        td_steal_kernel<<<grid, threads, steal_smem_bytes(warps), stream>>>(
+            d_in, d_out, count, s.d_pool, s.d_items, s.d_ready, s.d_epoch, s.item_capacity, s.d_state,
+            cfg.steal_grain, cfg.split_level, cfg.check_every, time_limit_ns(), cfg.tt_bits > 0 ? s.d_tt : nullptr,
+            cfg.tt_bits, cfg.restart_base, max_exp, count == 1 ? 4096u : 32768u);
+        TD_CHECK(cudaGetLastError());
+        td_finalize_kernel<<<std::max(1, std::min((count + 255) / 256, 2 * cfg.sms)), 256, 0, stream>>>(
+            s.d_pool, s.d_state, d_out, count);
     } else {
-        DeviceInfo &d = g_dev[s.device];
-        if (d.blocks_per_sm == 0) {
-            int b = 0;
-            TD_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, td_persistent_kernel<false>, threads, smem));
-            d.blocks_per_sm = std::max(1, b);
-        }
-        const int grid_max = d.sms * d.blocks_per_sm;
+        const int grid_max = cfg.sms * cfg.blocks_per_sm;
         const int grid = std::max(1, std::min(grid_max, (count + warps - 1) / warps));
         TD_CHECK(cudaMemsetAsync(s.d_ticket, 0, sizeof(int), stream));
         if (ordered)
-            td_persistent_kernel<true><<<grid, threads, smem, stream>>>(d_in, d_out, count, s.d_ticket, g_grain, max_exp, time_limit_ns());
+            td_persistent_kernel<true><<<grid, threads, smem, stream>>>(d_in, d_out, count, s.d_ticket, cfg.grain,
+                                                                        max_exp, time_limit_ns());
         else
-            td_persistent_kernel<false><<<grid, threads, smem, stream>>>(d_in, d_out, count, s.d_ticket, g_grain, max_exp, time_limit_ns());
+            td_persistent_kernel<false><<<grid, threads, smem, stream>>>(d_in, d_out, count, s.d_ticket, cfg.grain,
+                                                                         max_exp, time_limit_ns());
     }
     TD_CHECK(cudaGetLastError());
     if (flags & TD_FLAG_VERIFY) {
@@ -1312,7 +1372,14 @@ int noalloc_setup(int device, char *err, size_t errlen) {
     TD_CHECK_NA(cudaGetSymbolAddress(&ptr, td_noalloc_scratch));
     TD_CHECK_NA(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device));
     const size_t smem = smem_bytes(4);
-    TD_CHECK_NA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.steal_blocks, td_steal_kernel, 128, smem));
+    TD_CHECK_NA(cudaFuncSetAttribute(td_plain_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    TD_CHECK_NA(cudaFuncSetAttribute(td_plain_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    TD_CHECK_NA(cudaFuncSetAttribute(td_persistent_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    TD_CHECK_NA(cudaFuncSetAttribute(td_steal_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)steal_smem_bytes(4)));
+    TD_CHECK_NA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.steal_blocks, td_steal_kernel, 128,
+                                                              steal_smem_bytes(4)));
     TD_CHECK_NA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.persistent_blocks, td_persistent_kernel<true>,
                                                               128, smem));
     d.scratch = static_cast<uint8_t *>(ptr);
@@ -1370,15 +1437,33 @@ TD_API int td_search_batch_noalloc(int count, const td_instance *d_instances, td
         td_persistent_kernel<true><<<grid, threads, smem, st>>>(d_instances, d_results, count, ticket, 1, max_exp,
                                                                 limit);
     } else {
+        // the donation settings, read together (a concurrent td_configure_steal
+        // or td_configure_restart writes them under the same lock)
+        int grain, split_level, check_every;
+        uint32_t restart_base;
+        {
+            std::lock_guard<std::mutex> g(g_mu);
+            grain = g_steal_grain;
+            split_level = g_split_level;
+            check_every = g_check_every;
+            restart_base = g_restart_base;
+        }
         // counters and per-instance state start at zero on every call; items
         // are tagged with a fresh epoch so an earlier call's items never count
         TD_CHECK_NA(cudaMemsetAsync(pool, 0, sizeof(td_pool), st));
         TD_CHECK_NA(cudaMemsetAsync(state, 0, (size_t)count * sizeof(td_inst_state), st));
         td_epoch_kernel<<<1, 1, 0, st>>>(epoch);
-        const int grid = std::max(1, std::min(d.sms * std::max(1, d.steal_blocks), blocks_needed));
-        td_steal_kernel<<<grid, threads, smem, st>>>(d_instances, d_results, count, pool, items, ready, epoch,
-                                                     TD_NOALLOC_ITEMS, state, g_steal_grain, g_split_level,
-                                                     g_check_every, limit, nullptr, 0, g_restart_base, max_exp, 32768u);
+        // the whole resident grid (the scratch does not depend on its size):
+        // warps without an instance of their own take donated subtrees, so a
+        // small batch is spread over the GPU; a single search wakes its
+        // waiting warps sooner (backoff cap 4 us instead of 32 us)
+        const int grid = d.sms * std::max(1, d.steal_blocks);
+        td_steal_kernel<<<grid, threads, steal_smem_bytes(warps), st>>>(
+            d_instances, d_results, count, pool, items, ready, epoch, TD_NOALLOC_ITEMS, state, grain, split_level,
+            check_every, limit, nullptr, 0, restart_base, max_exp, count == 1 ? 4096u : 32768u);
+        TD_CHECK_NA(cudaGetLastError());
+        td_finalize_kernel<<<std::max(1, std::min((count + 255) / 256, 2 * d.sms)), 256, 0, st>>>(pool, state,
+                                                                                                d_results, count);
     }
     TD_CHECK_NA(cudaGetLastError());
     if (flags & TD_FLAG_VERIFY) {

@@ -674,6 +674,7 @@ __device__ __forceinline__ int td_donate(td_warp_smem &s, const td_donate_ctx &d
         for (int d = 0; d < TD_MAX_DEPTH; ++d) it.path[d] = d < lv ? s.path[d] : (d == lv ? (uint16_t)t : 0);
         int phys = slot;
         uint32_t tag = dc.epoch;
+        bool freed_ok = true;
         if (dc.ring) {
             phys = slot % dc.capacity;
             tag = td_ring_tag(slot);
@@ -684,15 +685,20 @@ __device__ __forceinline__ int td_donate(td_warp_smem &s, const td_donate_ctx &d
                 for (unsigned spin = 0; *(volatile uint32_t *)&dc.ready[phys] != freed; ++spin) {
                     if ((spin & 255u) == 0 && dc.deadline_ns && td_globaltimer() > dc.deadline_ns) {
                         atomicCAS(&dc.pool->error, 0, TD_ERR_TIMEOUT);
+                        freed_ok = false;
                         break;
                     }
                     __nanosleep(64);
                 }
             }
         }
-        dc.items[phys] = it;
-        __threadfence();
-        atomicExch(&dc.ready[phys], tag);
+        // after an expired wait the slot still belongs to an unread item: it
+        // is left alone, and this item's taker gives up at the deadline
+        if (freed_ok) {
+            dc.items[phys] = it;
+            __threadfence();
+            atomicExch(&dc.ready[phys], tag);
+        }
         ++slot;
     }
     s.pw[lv][lane] = make_uint4(W0, W1, W2, W3);

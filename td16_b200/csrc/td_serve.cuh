@@ -376,7 +376,15 @@ TD_API int td_serve_open(int device, unsigned ring_size, unsigned flags, double 
     if ((e = cudaMemsetAsync(sv->d_pool, 0, sizeof(td_pool), sv->stream)) != cudaSuccess) return fail(e, __LINE__);
     if ((e = cudaMemsetAsync(sv->d_ready, 0, sizeof(uint32_t) * sv->item_capacity, sv->stream)) != cudaSuccess)
         return fail(e, __LINE__);
-    const int warps = g_warps_per_block;
+    LaunchCfg cfg;
+    {
+        const int rc = launch_cfg(device, &cfg, err, errlen);
+        if (rc != TD_OK) {
+            server_free(sv);
+            return rc;
+        }
+    }
+    const int warps = cfg.warps;
     const size_t smem = smem_bytes(warps);
     int per_sm = 0;
     const bool ordered = flags & TD_FLAG_ORDERED;
@@ -389,7 +397,7 @@ TD_API int td_serve_open(int device, unsigned ring_size, unsigned flags, double 
     }
     const int grid = g_dev[device].sms * std::max(1, per_sm);
     sv->workers = grid * warps - 1;
-    const int tt_bits = ordered ? 0 : g_tt_bits;
+    const int tt_bits = ordered ? 0 : cfg.tt_bits;
     if (tt_bits > 0) {
         const size_t tt_bytes = ((size_t)grid * warps << tt_bits) * sizeof(uint64_t);
         if ((e = cudaMalloc(&sv->d_tt, tt_bytes)) != cudaSuccess) return fail(e, __LINE__);
@@ -398,13 +406,13 @@ TD_API int td_serve_open(int device, unsigned ring_size, unsigned flags, double 
     if (ordered)
         td_serve_kernel<true><<<grid, warps * 32, smem, sv->stream>>>(
             sv->d_ring, sv->d_res, sv->d_done, ring_size, sv->d_hctl, sv->d_ctl, sv->d_queue, sv->d_state,
-            sv->d_pool, sv->d_items, sv->d_ready, sv->item_capacity, g_serve_grain, g_serve_split_level,
-            g_serve_check_every, 0, limit_ns, nullptr, 0);
+            sv->d_pool, sv->d_items, sv->d_ready, sv->item_capacity, cfg.serve_grain, cfg.serve_split_level,
+            cfg.serve_check_every, 0, limit_ns, nullptr, 0);
     else
         td_serve_kernel<false><<<grid, warps * 32, smem, sv->stream>>>(
             sv->d_ring, sv->d_res, sv->d_done, ring_size, sv->d_hctl, sv->d_ctl, sv->d_queue, sv->d_state,
-            sv->d_pool, sv->d_items, sv->d_ready, sv->item_capacity, g_serve_grain, g_serve_split_level,
-            g_serve_check_every, 0, limit_ns, sv->d_tt, tt_bits);
+            sv->d_pool, sv->d_items, sv->d_ready, sv->item_capacity, cfg.serve_grain, cfg.serve_split_level,
+            cfg.serve_check_every, 0, limit_ns, sv->d_tt, tt_bits);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, __LINE__);
     *handle = sv;
     return TD_OK;

@@ -22,15 +22,10 @@ def oracle():
 
 @pytest.fixture(scope="session")
 def emu():
-    """Serial host emulation of the engine's warp algorithm (test only)."""
+    """Serial host emulation of the engine's warp algorithm (oracle/td_emu.cc, test only)."""
     import ctypes as C
-    src = os.path.join(ROOT, "tests", "emu", "td_emu.cc")
-    lib = os.path.join(ROOT, "tests", "emu", "libtdemu.so")
-    if not os.path.exists(lib) or os.path.getmtime(lib) < max(
-            os.path.getmtime(src), os.path.getmtime(os.path.join(ROOT, "td16_b200", "csrc", "td_core.cuh"))):
-        subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fno-fast-math", "-ffp-contract=off",
-                        "-o", lib, src], check=True)
-    return C.CDLL(lib)
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+    return C.CDLL(os.path.join(ROOT, "oracle", "libtdemu.so"))
 
 
 @pytest.fixture(scope="session")

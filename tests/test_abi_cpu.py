@@ -130,3 +130,13 @@ def test_configuration_arguments_are_checked(td):
     assert lib.td_configure_serve(1, 2, 32) == td._lib.OK
     with pytest.raises(td.TdError):
         td._lib.configure_table(3)
+
+
+def test_oracle_generator_matches_the_engine_bit_for_bit(td, oracle):
+    """The oracle's restatement of the seeded generator (used where the engine
+    library must not be loaded) gives the engine's td_synth_perms output."""
+    for args in ((2, 1 << 15, 16, 16, 50, 1, 4), (1, 1 << 14, 11, 13, 25, 1, 3), (0, 4096, 10, 10, 0, 0, 0),
+                 (3, 4096, 8, 16, 0, 0, 0), (7, 4096, 1, 16, 37, 0, 5), (9, 512, 16, 16, 100, 4, 4)):
+        p_o, n_o = oracle.synth_perms(*args)
+        p_t, n_t = td.synth_perms(*args)
+        assert (p_o == p_t).all() and (n_o == n_t).all(), args
