@@ -107,6 +107,17 @@ int td_search_ordered(int slot, const uint8_t *beta, const uint8_t *omega, int n
                       int full_sorting, int16_t *out_ijk, int *out_depth,
                       char *err, size_t errlen);
 
+/* How td_search and td_search_ordered run (no counterpart in the reference,
+ * which launches per call).  mode 1 (default): through one resident serving
+ * launch per device; the calling thread writes its request into pinned,
+ * device-mapped memory and polls for the result, so a search costs no CUDA
+ * API call.  The launch holds half of each SM's block slots while per-call
+ * searches run; batch entry points stop it first when none is in flight.
+ * mode 0: one launch per call on the slot's stream.  rotate_after_s > 0 sets
+ * the age at which a server launch is replaced by a fresh one (default 300;
+ * every wait of a launch is bounded by its deadline); 0 keeps the setting. */
+int td_configure_percall(int mode, double rotate_after_s);
+
 int td_slot_count(void);
 int td_slot_device(int slot);           /* -1 for an invalid slot */
 void *td_slot_stream(int slot);         /* cudaStream_t of the slot */
@@ -172,6 +183,23 @@ int td_synth_perms(uint64_t seed, int count, int n_min, int n_max, int hard_pct,
 int td_search_batch(int slot, int count, const td_instance *instances,
                     td_result *results, unsigned flags,
                     uint64_t max_expansions, td_batch_stats *stats, char *err,
+                    size_t errlen);
+
+/* Many reference pairs per call: the batch form of td_search, for a case
+ * producer that hands pairs over in groups instead of one blocking call per
+ * pair (the enumerator's Consumer<CyclicTargetPair>,
+ * DirectTwistedBraceletGenerator.java:105-156, calls searchForSortingSeq once
+ * per pair through GPUSortingSearch.java:134-162).  Pair i: beta/omega at
+ * stride 17 bytes, n[i] <= 17 symbols, init[i], min_rate[i], max_moves[i],
+ * full[i].  flags: 0 or TD_FLAG_ORDERED.  Per pair: status[i] is TD_OK
+ * (found; depth[i] position triples at out_ijk[27 i + 3 d ..]),
+ * TD_NOT_FOUND (also for n < 3), or the per-call error class
+ * (TD_INVALID_ARG, TD_OVERFLOW, TD_TIMEOUT).  Returns TD_OK when the batch
+ * ran, else the error of the whole call (invalid slot, CUDA error). */
+int td_search_pairs(int slot, int count, const uint8_t *beta, const uint8_t *omega,
+                    const uint8_t *n, const int32_t *init, const float *min_rate,
+                    const int32_t *max_moves, const uint8_t *full, unsigned flags,
+                    int32_t *status, int32_t *depth, int16_t *out_ijk, char *err,
                     size_t errlen);
 
 /* Device buffers; enqueues on `stream` (a cudaStream_t, or NULL for the

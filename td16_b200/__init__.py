@@ -7,4 +7,4 @@ for the search (``host``).
 from . import _lib  # noqa: F401
 from ._lib import (INSTANCE_DTYPE, RESULT_DTYPE, TdError, init_slots, destroy, search,  # noqa: F401
                    search_batch, prepare_pairs, prepare_perms, synth_perms, unpack_moves)
-from .host import GPUSortingSearch, GpuDeviceLayout, GpuSearchStats  # noqa: F401
+from .host import GPUSortingSearch, GpuDeviceLayout, GpuSearchStats, PairBatcher  # noqa: F401

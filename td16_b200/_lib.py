@@ -57,7 +57,7 @@ EXPORTS = ["td_init_slots", "td_search", "td_search_ordered", "td_slot_count", "
            "td_codec_key", "td_codec_value", "td_codec_decode_key", "td_codec_decode_value",
            "td_replay_symbols_device", "td_cert_writer_open", "td_cert_writer_enqueue", "td_cert_writer_close",
            "td_serve_open", "td_serve_workers", "td_serve_submit", "td_serve_poll", "td_serve_close",
-           "td_serve_open_loop", "td_cert_writer_enqueue_batch", "td_cert_read_file", "td_pairs_from_perms", "td_batch_graph_create", "td_batch_graph_launch", "td_batch_graph_destroy"]
+           "td_serve_open_loop", "td_configure_percall", "td_search_pairs", "td_cert_writer_enqueue_batch", "td_cert_read_file", "td_pairs_from_perms", "td_batch_graph_create", "td_batch_graph_launch", "td_batch_graph_destroy"]
 
 
 def lib():
@@ -93,6 +93,8 @@ def lib():
     L.td_configure_table.argtypes = [C.c_int]
     L.td_configure_restart.argtypes = [C.c_int]
     L.td_set_time_limit.argtypes = [C.c_double]
+    L.td_configure_percall.argtypes = [C.c_int, C.c_double]
+    L.td_search_pairs.argtypes = [C.c_int, C.c_int] + [vp] * 7 + [C.c_uint] + [vp] * 3 + [cp, sz]
     L.td_codec_key.argtypes = [vp, C.c_int, vp, C.c_int]
     L.td_codec_value.argtypes = [vp, C.c_int, vp, C.c_int]
     L.td_codec_decode_key.argtypes = [vp, C.c_int, C.c_int, vp]
@@ -163,6 +165,27 @@ def search(slot: int, beta, omega, initial_even_cycles: int, min_rate: float, ma
            out, C.byref(depth), err, 512)
     check(rc, err)
     return [(out[3 * d], out[3 * d + 1], out[3 * d + 2]) for d in range(depth.value)]
+
+
+def search_pairs(slot: int, beta, omega, n, init, min_rate, max_moves, full=1, ordered: bool = False):
+    """Many reference pairs in one call (td_search_pairs).  beta/omega
+    uint8[count, 17]; the rest per pair or broadcast.  Returns (status
+    int32[count] with the per-call codes, depth int32[count], position
+    triples int16[count, 9, 3])."""
+    count = int(beta.shape[0])
+    beta = np.ascontiguousarray(beta, np.uint8)
+    omega = np.ascontiguousarray(omega, np.uint8)
+    bc = lambda v, dt: np.ascontiguousarray(np.broadcast_to(v, (count,)), dt)  # noqa: E731
+    arrs = [bc(n, np.uint8), bc(init, np.int32), bc(min_rate, np.float32), bc(max_moves, np.int32),
+            bc(full, np.uint8)]
+    status = np.zeros(count, np.int32)
+    depth = np.zeros(count, np.int32)
+    moves = np.zeros((count, 9, 3), np.int16)
+    err = C.create_string_buffer(512)
+    rc = lib().td_search_pairs(int(slot), count, _ptr(beta), _ptr(omega), *[_ptr(a) for a in arrs],
+                               FLAG_ORDERED if ordered else 0, _ptr(status), _ptr(depth), _ptr(moves), err, 512)
+    check(rc, err)
+    return status, depth, moves
 
 
 def prepare_pairs(beta: np.ndarray, omega: np.ndarray, n, init, min_rate, max_moves, full) -> np.ndarray:
@@ -274,6 +297,13 @@ def configure_restart(base: int) -> None:
     """Restart budgets of free-order batch searches: base x Luby sequence, 0 = none."""
     if lib().td_configure_restart(int(base)) != OK:
         raise TdError(INVALID_ARG, "restart base must be 0 or >= 16")
+
+
+def configure_percall(mode: int, rotate_after_s: float = 0.0) -> None:
+    """Per-call searches: 1 through the device's resident server (default),
+    0 one launch per call; rotate_after_s > 0 sets the server's rotation age."""
+    if lib().td_configure_percall(int(mode), float(rotate_after_s)) != OK:
+        raise TdError(INVALID_ARG, "per-call mode must be 0 or 1 and the rotation age >= 0")
 
 
 def configure_serve(grain: int, split_level: int, check_every: int) -> None:

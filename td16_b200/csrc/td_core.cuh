@@ -44,7 +44,9 @@ struct td_instance {
     uint8_t n_symbols;  // N
     uint8_t offset;     // pinned position of the caller's beta[0]
     uint8_t max_moves;  // 1..9
-    uint8_t packed;     // bits 0-4: initialEvenCycles, bit 7: fullSorting
+    uint8_t packed;     // bits 0-4: initialEvenCycles, bit 7: fullSorting,
+                        // bit 6: reference order (set by the engine on requests
+                        // to its per-call server only)
 };
 
 // One search result: 32 bytes.
@@ -80,6 +82,7 @@ TD_HD uint64_t td_low_nibbles(int count) {  // mask of the lowest `count` nibble
 
 TD_HD int td_inst_init(const td_instance &x) { return x.packed & 31; }
 TD_HD int td_inst_full(const td_instance &x) { return (x.packed >> 7) & 1; }
+#define TD_PACKED_ORDERED 0x40
 
 // Apply the caller-position move (i,j,k) to the pinned state (L, off).
 // The three cut points are pinned positions P,Q,R in cyclic order; rotated so

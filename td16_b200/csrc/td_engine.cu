@@ -656,7 +656,14 @@ void release_slot(Slot &s) {
     s = Slot{};
 }
 
+// the per-call server (td_percall.cuh)
+void percall_shutdown();
+void percall_park(int device);
+int percall_search(int device, const td_instance &x, td_result *out, char *err, size_t errlen);
+extern std::atomic<int> g_percall_mode;
+
 void destroy_all() {
+    percall_shutdown();
     for (auto &s : g_slots) release_slot(s);
     g_slots.clear();
 }
@@ -754,9 +761,18 @@ int search_one(int slot, const uint8_t *beta, const uint8_t *omega, int n, int i
                int max_moves, int full, int16_t *out_ijk, int *out_depth, unsigned flags, char *err,
                size_t errlen) {
     if (out_depth) *out_depth = 0;
+    // the reference's order of checks: null arrays, the slot
+    // (jni_sorter.cu:59-92), then n, the depth and n < 3
+    // (sorting_search.cu:821-827)
     if (!beta || !omega) {
         set_err(err, errlen, "beta and omega must not be null");
         return TD_INVALID_ARG;
+    }
+    Slot *s;
+    {
+        std::lock_guard<std::mutex> g(g_mu);
+        s = get_slot(slot, err, errlen);
+        if (!s) return TD_INVALID_ARG;
     }
     if (n > TD_MAX_N) {
         set_err(err, errlen, "performGpuSortingSearch: n exceeds MAX_N");
@@ -766,32 +782,35 @@ int search_one(int slot, const uint8_t *beta, const uint8_t *omega, int n, int i
         set_err(err, errlen, "performGpuSortingSearch: invalid maximumDepth");
         return TD_INVALID_ARG;
     }
-    Slot *s;
-    {
-        std::lock_guard<std::mutex> g(g_mu);
-        s = get_slot(slot, err, errlen);
-        if (!s) return TD_INVALID_ARG;
-    }
     if (td_triple_count(n) == 0) return TD_NOT_FOUND_RC;
     td_instance x;
     if (td_prepare_pair(beta, omega, n, init, min_rate, max_moves, full, &x) != 0) {
         set_err(err, errlen, "beta/omega are not permutations whose product omega.beta is an n-cycle");
         return TD_INVALID_ARG;
     }
-    std::lock_guard<std::mutex> g(*s->mu);
-    TD_CHECK(cudaSetDevice(s->device));
-    *s->h_inst = x;
-    TD_CHECK(cudaMemcpyAsync(s->d_inst, s->h_inst, sizeof(td_instance), cudaMemcpyHostToDevice, s->stream));
-    // free order: the donation engine over the slot's share of the GPU (as the
-    // reference gives each slot SMs x resident blocks / slots queues,
-    // sorting_search.cu:740-752); the reference order keeps one warp
-    const unsigned how = (flags & TD_FLAG_ORDERED) ? (flags | TD_FLAG_PLAIN) : flags;
-    int rc = launch_batch(*s, 1, s->d_inst, s->d_res, how, 0, s->stream, err, errlen);
-    if (rc != TD_OK) return rc;
-    TD_CHECK(cudaMemcpyAsync(s->h_res, s->d_res, sizeof(td_result), cudaMemcpyDeviceToHost, s->stream));
-    TD_CHECK(cudaEventRecord(s->done, s->stream));
-    TD_CHECK(cudaEventSynchronize(s->done));
-    const td_result r = *s->h_res;
+    td_result r;
+    if (g_percall_mode.load(std::memory_order_relaxed) == 1) {
+        // the device's resident per-call server: no CUDA call per search
+        if (flags & TD_FLAG_ORDERED) x.packed |= TD_PACKED_ORDERED;
+        const int rc = percall_search(s->device, x, &r, err, errlen);
+        if (rc != TD_OK) return rc;
+    } else {
+        std::lock_guard<std::mutex> g(*s->mu);
+        TD_CHECK(cudaSetDevice(s->device));
+        *s->h_inst = x;
+        TD_CHECK(cudaMemcpyAsync(s->d_inst, s->h_inst, sizeof(td_instance), cudaMemcpyHostToDevice, s->stream));
+        // free order: the donation engine over the slot's share of the GPU (as
+        // the reference gives each slot SMs x resident blocks / slots queues,
+        // sorting_search.cu:740-752); the reference order keeps one warp
+        const unsigned how = (flags & TD_FLAG_ORDERED) ? (flags | TD_FLAG_PLAIN) : flags;
+        percall_park(s->device);
+        int rc = launch_batch(*s, 1, s->d_inst, s->d_res, how, 0, s->stream, err, errlen);
+        if (rc != TD_OK) return rc;
+        TD_CHECK(cudaMemcpyAsync(s->h_res, s->d_res, sizeof(td_result), cudaMemcpyDeviceToHost, s->stream));
+        TD_CHECK(cudaEventRecord(s->done, s->stream));
+        TD_CHECK(cudaEventSynchronize(s->done));
+        r = *s->h_res;
+    }
     if (r.status == TD_FOUND) {
         for (int d = 0; d < r.depth; ++d) {
             out_ijk[3 * d + 0] = (int16_t)(r.moves[d] & 31);
@@ -1127,6 +1146,7 @@ TD_API int td_search_batch_device(int slot, int count, const td_instance *d_in, 
         set_err(err, errlen, "invalid batch arguments");
         return TD_INVALID_ARG;
     }
+    percall_park(s->device);
     std::lock_guard<std::mutex> g(*s->mu);
     TD_CHECK(cudaSetDevice(s->device));
     cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
@@ -1149,6 +1169,7 @@ TD_API int td_search_batch(int slot, int count, const td_instance *in, td_result
         if (stats) std::memset(stats, 0, sizeof *stats);
         return TD_OK;
     }
+    percall_park(s->device);
     std::lock_guard<std::mutex> g(*s->mu);
     TD_CHECK(cudaSetDevice(s->device));
     const size_t need = (size_t)count * (sizeof(td_instance) + sizeof(td_result));
@@ -1200,6 +1221,82 @@ TD_API int td_search_batch(int slot, int count, const td_instance *in, td_result
         stats->found = c.found;
         stats->not_found = c.not_found;
         stats->errors = c.errors;
+    }
+    return TD_OK;
+}
+
+// Many reference pairs in one call: the batch form of td_search for a case
+// producer that hands over pairs in groups (the enumerator's
+// Consumer<CyclicTargetPair>, DirectTwistedBraceletGenerator.java:105-156,
+// feeds one pair per call today).  Pair i: beta/omega at stride 17, n[i]
+// symbols, init[i], min_rate[i], max_moves[i], full[i].  Outputs per pair:
+// status[i] (TD_OK found, TD_NOT_FOUND, or the per-call error class:
+// TD_INVALID_ARG, TD_OVERFLOW, TD_TIMEOUT), depth[i] and the position
+// triples at out_ijk[27 i ..].  Returns TD_OK when the batch ran (the pair
+// statuses say the rest), else the error of the whole call.
+TD_API int td_search_pairs(int slot, int count, const uint8_t *beta, const uint8_t *omega, const uint8_t *n,
+                           const int32_t *init, const float *min_rate, const int32_t *max_moves,
+                           const uint8_t *full, unsigned flags, int32_t *status, int32_t *depth, int16_t *out_ijk,
+                           char *err, size_t errlen) {
+    if (count < 0 || (count > 0 && (!beta || !omega || !n || !init || !min_rate || !max_moves || !full ||
+                                    !status || !depth || !out_ijk))) {
+        set_err(err, errlen, "invalid batch arguments");
+        return TD_INVALID_ARG;
+    }
+    std::vector<td_instance> inst;
+    std::vector<int> index;  // batch position -> pair
+    inst.reserve(count);
+    index.reserve(count);
+    for (int i = 0; i < count; ++i) {
+        depth[i] = 0;
+        for (int q = 0; q < 27; ++q) out_ijk[27 * (size_t)i + q] = 0;
+        if (n[i] > TD_MAX_N || max_moves[i] <= 0 || max_moves[i] > TD_MAX_DEPTH) {
+            status[i] = TD_INVALID_ARG;
+            continue;
+        }
+        if (td_triple_count(n[i]) == 0) {
+            status[i] = TD_NOT_FOUND_RC;
+            continue;
+        }
+        td_instance x;
+        if (td_prepare_pair(beta + 17 * (size_t)i, omega + 17 * (size_t)i, n[i], init[i], min_rate[i],
+                            max_moves[i], full[i], &x) != 0) {
+            status[i] = TD_INVALID_ARG;
+            continue;
+        }
+        inst.push_back(x);
+        index.push_back(i);
+    }
+    if (inst.empty()) {
+        Slot *s;
+        std::lock_guard<std::mutex> g(g_mu);
+        s = get_slot(slot, err, errlen);
+        return s ? TD_OK : TD_INVALID_ARG;
+    }
+    std::vector<td_result> res(inst.size());
+    const int rc = td_search_batch(slot, (int)inst.size(), inst.data(), res.data(), flags & TD_FLAG_ORDERED, 0,
+                                   nullptr, err, errlen);
+    if (rc != TD_OK) return rc;
+    for (size_t b = 0; b < res.size(); ++b) {
+        const int i = index[b];
+        const td_result &r = res[b];
+        if (r.status == TD_FOUND) {
+            status[i] = TD_OK;
+            depth[i] = r.depth;
+            for (int d = 0; d < r.depth; ++d) {
+                out_ijk[27 * (size_t)i + 3 * d + 0] = (int16_t)(r.moves[d] & 31);
+                out_ijk[27 * (size_t)i + 3 * d + 1] = (int16_t)((r.moves[d] >> 5) & 31);
+                out_ijk[27 * (size_t)i + 3 * d + 2] = (int16_t)((r.moves[d] >> 10) & 31);
+            }
+        } else if (r.status == TD_NOT_FOUND) {
+            status[i] = TD_NOT_FOUND_RC;
+        } else if (r.status == TD_ERR_BUDGET) {
+            status[i] = TD_OVERFLOW;
+        } else if (r.status == TD_ERR_TIMEOUT) {
+            status[i] = TD_TIMEOUT;
+        } else {
+            status[i] = TD_INVALID_ARG;
+        }
     }
     return TD_OK;
 }
@@ -1498,6 +1595,7 @@ TD_API int td_batch_graph_create(int slot, int count, const td_instance *d_in, t
         set_err(err, errlen, "invalid graph arguments");
         return TD_INVALID_ARG;
     }
+    percall_park(s->device);
     std::lock_guard<std::mutex> g(*s->mu);
     TD_CHECK(cudaSetDevice(s->device));
     // one eager launch sizes the slot's scratch outside the capture
@@ -1530,6 +1628,7 @@ TD_API int td_batch_graph_create(int slot, int count, const td_instance *d_in, t
 TD_API int td_batch_graph_launch(void *graph, void *stream, char *err, size_t errlen) {
     auto *bg = static_cast<BatchGraph *>(graph);
     if (!bg) return TD_INVALID_ARG;
+    percall_park(bg->device);
     TD_CHECK(cudaSetDevice(bg->device));
     TD_CHECK(cudaGraphLaunch(bg->exec, (cudaStream_t)stream));
     return TD_OK;
@@ -1546,3 +1645,4 @@ TD_API int td_batch_graph_destroy(void *graph) {
 }
 
 #include "td_serve.cuh"
+#include "td_percall.cuh"

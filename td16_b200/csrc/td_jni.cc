@@ -1,12 +1,19 @@
-// td_jni.cc -- JNI shim: class br.unb.cic.tdp.base.GPUSortingSearch binds these
-// two natives (GPUSortingSearch.java:115-117) from library td16_jni; both
-// forward to the C ABI of libtd16b200.so.  A non-OK status becomes a
-// java.lang.RuntimeException carrying the engine's message, as in
-// emitter/src/native/jni/jni_sorter.cu:15-22, 111-115.  Built only where a
-// JDK's jni.h exists (td16_b200/build.py).
+// td_jni.cc -- JNI shim: class br.unb.cic.tdp.base.GPUSortingSearch binds
+// these natives from library td16_jni; each forwards to the C ABI of
+// libtd16b200.so.
+//   initSlots, searchForSortingSeq   the reference's two natives
+//                                    (GPUSortingSearch.java:115-117,
+//                                    emitter/src/native/jni/jni_sorter.cu:24-117)
+//   searchForSortingSeqBatch         an addition for a case producer that
+//                                    hands over pairs in groups
+// A non-OK status becomes a java.lang.RuntimeException carrying the engine's
+// message, as jni_sorter.cu:15-22,111-115 does for every C++ exception.  Built
+// only where a JDK's jni.h exists (td16_b200/build.py); the tests compile it
+// against a minimal hand-written jni.h and a fake JNIEnv (tests/jni/).
 #include <jni.h>
 
 #include <cstdint>
+#include <cstdio>
 #include <vector>
 
 #include "td16_b200.h"
@@ -39,6 +46,21 @@ extern "C" JNIEXPORT void JNICALL Java_br_unb_cic_tdp_base_GPUSortingSearch_init
     if (rc != TD_OK) throw_runtime(env, err[0] ? err : "initSlots failed");
 }
 
+// int[depth][3] of position triples (empty, not null, without a witness)
+static jobjectArray moves_array(JNIEnv *env, const int16_t *ijk, int depth) {
+    jclass int_array = env->FindClass("[I");
+    jobjectArray outer = env->NewObjectArray(depth, int_array, nullptr);
+    for (int d = 0; d < depth; ++d) {
+        const jint move[3] = {ijk[3 * d], ijk[3 * d + 1], ijk[3 * d + 2]};
+        jintArray inner = env->NewIntArray(3);
+        env->SetIntArrayRegion(inner, 0, 3, move);
+        env->SetObjectArrayElement(outer, d, inner);
+        env->DeleteLocalRef(inner);
+    }
+    env->DeleteLocalRef(int_array);
+    return outer;
+}
+
 extern "C" JNIEXPORT jobjectArray JNICALL Java_br_unb_cic_tdp_base_GPUSortingSearch_searchForSortingSeq(
     JNIEnv *env, jclass, jbyteArray beta, jbyteArray omega, jint initial_even_cycles, jfloat min_rate,
     jint max_moves, jboolean full_sorting, jint slot) {
@@ -65,15 +87,100 @@ extern "C" JNIEXPORT jobjectArray JNICALL Java_br_unb_cic_tdp_base_GPUSortingSea
         throw_runtime(env, err[0] ? err : "GPU sorting search failed");
         return nullptr;
     }
-    jclass int_array = env->FindClass("[I");
-    jobjectArray outer = env->NewObjectArray(depth, int_array, nullptr);
-    for (int d = 0; d < depth; ++d) {
-        const jint move[3] = {ijk[3 * d], ijk[3 * d + 1], ijk[3 * d + 2]};
-        jintArray inner = env->NewIntArray(3);
-        env->SetIntArrayRegion(inner, 0, 3, move);
-        env->SetObjectArrayElement(outer, d, inner);
+    return moves_array(env, ijk, rc == TD_OK ? depth : 0);
+}
+
+// The batch form: pair p is (betas[p], omegas[p], initialEvenCycles[p],
+// minRates[p], maxMoves[p], fullSorting[p]); returns int[count][][3], entry p
+// as searchForSortingSeq would return it.  A pair that searchForSortingSeq
+// would reject raises the same RuntimeException class, prefixed with the
+// pair's index, and the call returns null.
+extern "C" JNIEXPORT jobjectArray JNICALL Java_br_unb_cic_tdp_base_GPUSortingSearch_searchForSortingSeqBatch(
+    JNIEnv *env, jclass, jobjectArray betas, jobjectArray omegas, jintArray initial_even_cycles,
+    jfloatArray min_rates, jintArray max_moves, jbooleanArray full_sorting, jint slot) {
+    if (!betas || !omegas || !initial_even_cycles || !min_rates || !max_moves || !full_sorting) {
+        throw_runtime(env, "batch arrays must not be null");
+        return nullptr;
+    }
+    const jsize count = env->GetArrayLength(betas);
+    if (env->GetArrayLength(omegas) != count || env->GetArrayLength(initial_even_cycles) != count ||
+        env->GetArrayLength(min_rates) != count || env->GetArrayLength(max_moves) != count ||
+        env->GetArrayLength(full_sorting) != count) {
+        throw_runtime(env, "batch arrays must have equal lengths");
+        return nullptr;
+    }
+    const size_t c = count > 0 ? (size_t)count : 1;
+    std::vector<uint8_t> b(17 * c, 0), o(17 * c, 0), n(c, 0), full(c, 0);
+    std::vector<int32_t> init(c, 0), maxd(c, 0), status(c, 0), depth(c, 0);
+    std::vector<float> rate(c, 0.f);
+    std::vector<int16_t> ijk(27 * c, 0);
+    for (jsize p = 0; p < count; ++p) {
+        jbyteArray bp = (jbyteArray)env->GetObjectArrayElement(betas, p);
+        jbyteArray op = (jbyteArray)env->GetObjectArrayElement(omegas, p);
+        if (!bp || !op) {
+            char msg[96];
+            std::snprintf(msg, sizeof msg, "pair %d: beta and omega must not be null", (int)p);
+            throw_runtime(env, msg);
+            return nullptr;
+        }
+        const jsize len = env->GetArrayLength(bp);
+        if (env->GetArrayLength(op) != len || len > 17) {
+            char msg[96];
+            std::snprintf(msg, sizeof msg, "pair %d: %s", (int)p,
+                          len > 17 ? "performGpuSortingSearch: n exceeds MAX_N"
+                                   : "beta and omega must have equal lengths");
+            throw_runtime(env, msg);
+            return nullptr;
+        }
+        if (len > 0) {
+            env->GetByteArrayRegion(bp, 0, len, reinterpret_cast<jbyte *>(&b[17 * (size_t)p]));
+            env->GetByteArrayRegion(op, 0, len, reinterpret_cast<jbyte *>(&o[17 * (size_t)p]));
+        }
+        n[p] = (uint8_t)len;
+        env->DeleteLocalRef(bp);
+        env->DeleteLocalRef(op);
+    }
+    if (count > 0) {
+        std::vector<jint> ji(c), jm(c);
+        std::vector<jboolean> jf(c);
+        env->GetIntArrayRegion(initial_even_cycles, 0, count, ji.data());
+        env->GetFloatArrayRegion(min_rates, 0, count, rate.data());
+        env->GetIntArrayRegion(max_moves, 0, count, jm.data());
+        env->GetBooleanArrayRegion(full_sorting, 0, count, jf.data());
+        for (size_t p = 0; p < (size_t)count; ++p) {
+            init[p] = ji[p];
+            maxd[p] = jm[p];
+            full[p] = jf[p] ? 1 : 0;
+        }
+    }
+    char err[512] = {0};
+    const int rc = td_search_pairs((int)slot, (int)count, b.data(), o.data(), n.data(), init.data(), rate.data(),
+                                   maxd.data(), full.data(), 0u, status.data(), depth.data(), ijk.data(), err,
+                                   sizeof err);
+    if (rc != TD_OK) {
+        throw_runtime(env, err[0] ? err : "GPU sorting search failed");
+        return nullptr;
+    }
+    for (jsize p = 0; p < count; ++p) {
+        const char *what = nullptr;
+        if (status[p] == TD_OVERFLOW) what = "GPU sorting search queue overflow";
+        else if (status[p] == TD_TIMEOUT) what = "GPU sorting search deadline reached";
+        else if (status[p] == TD_INVALID_ARG) what = "performGpuSortingSearch: invalid input";
+        else if (status[p] != TD_OK && status[p] != TD_NOT_FOUND) what = "GPU sorting search failed";
+        if (what) {
+            char msg[160];
+            std::snprintf(msg, sizeof msg, "pair %d: %s", (int)p, what);
+            throw_runtime(env, msg);
+            return nullptr;
+        }
+    }
+    jclass moves_class = env->FindClass("[[I");
+    jobjectArray outer = env->NewObjectArray(count, moves_class, nullptr);
+    for (jsize p = 0; p < count; ++p) {
+        jobjectArray inner = moves_array(env, &ijk[27 * (size_t)p], status[p] == TD_OK ? depth[p] : 0);
+        env->SetObjectArrayElement(outer, p, inner);
         env->DeleteLocalRef(inner);
     }
-    env->DeleteLocalRef(int_array);
+    env->DeleteLocalRef(moves_class);
     return outer;
 }

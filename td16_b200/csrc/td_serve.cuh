@@ -46,19 +46,32 @@ __device__ __forceinline__ void td_serve_record(td_serve_dev_ctl *dctl, const td
     atomicCAS(&dctl->error, 0, TD_ERR_TIMEOUT);
 }
 
+// Move order of a serving launch: every request in the free order, every
+// request in the reference order, or per request (TD_PACKED_ORDERED in the
+// request's packed byte; the per-call server of td_search and
+// td_search_ordered).
+#define TD_SERVE_FREE 0
+#define TD_SERVE_ORDERED 1
+#define TD_SERVE_PER_REQUEST 2
+
 // Worker warps take fresh requests in arrival order and, in free order, also
 // donated subtrees of requests that others are searching (the batch engine's
 // donation scheme over a ring of items), so one hard request does not hold a
 // single warp for its whole search.  The warp that finishes a request last
-// writes its result and stamps done[slot] = request + 1.
-template <bool ORDERED>
+// writes its result and stamps done[slot] = request + 1.  A free-order request
+// restarts with another child order after restart_base x Luby expansions (0:
+// never), as in the batch engine.  Each request's search also ends
+// request_limit_ns after it starts (0: only the launch deadline).
+template <int MODE>
 __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *ring, td_result *results,
                                                       volatile unsigned long long *done, unsigned ring_size,
                                                       td_serve_host_ctl *hctl, td_serve_dev_ctl *dctl,
                                                       td_instance *queue, td_inst_state *state, td_pool *pool,
                                                       td_item *items, uint32_t *ready, int item_capacity,
                                                       int grain, int max_level, int check_every, uint64_t max_exp,
-                                                      uint64_t time_limit_ns, uint64_t *tt, int tt_bits) {
+                                                      uint64_t time_limit_ns, uint64_t *tt, int tt_bits,
+                                                      uint32_t restart_base, uint64_t request_limit_ns) {
+    constexpr bool ALL_ORDERED = MODE == TD_SERVE_ORDERED;
     extern __shared__ __align__(16) uint8_t td_smem[];
     const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint8_t *lut = td_smem;
@@ -107,7 +120,7 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
     lim.max_expansions = max_exp ? max_exp : ~0ull;
     lim.deadline_ns = deadline;
     lim.abort_flag = nullptr;
-    lim.tt = (!ORDERED && tt) ? tt + ((size_t)(blockIdx.x * warps + warp) << tt_bits) : nullptr;
+    lim.tt = (!ALL_ORDERED && tt) ? tt + ((size_t)(blockIdx.x * warps + warp) << tt_bits) : nullptr;
     lim.tt_bits = tt_bits;
     lim.restart_base = 0;  // serving searches are not restarted
     td_donate_ctx dc;
@@ -130,7 +143,7 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
             // donated subtrees of requests in flight come before fresh
             // requests: under load, fresh arrivals would otherwise keep every
             // warp busy while a started request waits for its subtrees
-            if (!ORDERED) {
+            if (!ALL_ORDERED) {
                 const int P = *(volatile int *)&pool->produced;
                 int C = *(volatile int *)&pool->consumed;
                 while (C < P) {
@@ -179,6 +192,7 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
         r.found_move = 0;
         r.expansions = 0;
         bool run = false;
+        bool ord = ALL_ORDERED;  // this unit's move order (donated subtrees: free)
         int d0 = 0;
         if (kind == 1) {
             const unsigned slot = (unsigned)(req % ring_size);
@@ -203,7 +217,9 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
                     atomicAdd(&dctl->served, 1ull);
                 }
             } else {
-                td_setup_root<ORDERED>(s, x, code, codeN);
+                if (MODE == TD_SERVE_PER_REQUEST) ord = (x.packed & TD_PACKED_ORDERED) != 0;
+                if (ord) td_setup_root<true>(s, x, code, codeN);
+                else td_setup_root<false>(s, x, code, codeN);
                 run = true;
             }
         } else {
@@ -238,7 +254,7 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
                 const unsigned slot = (unsigned)(req % ring_size);
                 const uint4 v = __ldcg(reinterpret_cast<const uint4 *>(&queue[slot]));
                 const td_instance x = *reinterpret_cast<const td_instance *>(&v);
-                td_setup_root<ORDERED>(s, x, code, codeN);
+                td_setup_root<false>(s, x, code, codeN);
                 d0 = it.depth;
                 if (lane == 0) {
                     s.L[d0] = it.L;
@@ -263,7 +279,12 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
             const td_instance x = *reinterpret_cast<const td_instance *>(&v);
             dc.inst = (uint32_t)req;
             dc.state = &state[slot];
-            r = td_dfs<ORDERED>(s, lut, code, x.n_symbols, x.max_moves, d0, lim, ORDERED ? nullptr : &dc);
+            td_search_limits ulim = lim;
+            if (request_limit_ns) ulim.deadline_ns = min(deadline, td_globaltimer() + request_limit_ns);
+            // a fresh request may restart; a donated subtree is searched once
+            ulim.restart_base = kind == 1 ? restart_base : 0;
+            if (ord) r = td_dfs<true>(s, lut, code, x.n_symbols, x.max_moves, d0, ulim, nullptr);
+            else r = td_dfs<false>(s, lut, code, x.n_symbols, x.max_moves, d0, ulim, &dc);
             if (td_finish_unit(r, &state[slot], &results[slot], s.path) && lane == 0) {
                 done[slot] = (unsigned long long)req + 1ull;
                 atomicAdd(&dctl->served, 1ull);
@@ -340,6 +361,7 @@ TD_API int td_serve_open(int device, unsigned ring_size, unsigned flags, double 
         const int rc = ensure_device(device, err, errlen);
         if (rc != TD_OK) return rc;
     }
+    percall_park(device);
     auto *sv = new Server();
     sv->device = device;
     sv->flags = flags;
@@ -389,11 +411,11 @@ TD_API int td_serve_open(int device, unsigned ring_size, unsigned flags, double 
     int per_sm = 0;
     const bool ordered = flags & TD_FLAG_ORDERED;
     if (ordered) {
-        if ((e = cudaFuncSetAttribute(td_serve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) return fail(e, __LINE__);
-        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, td_serve_kernel<true>, warps * 32, smem)) != cudaSuccess) return fail(e, __LINE__);
+        if ((e = cudaFuncSetAttribute(td_serve_kernel<TD_SERVE_ORDERED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) return fail(e, __LINE__);
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, td_serve_kernel<TD_SERVE_ORDERED>, warps * 32, smem)) != cudaSuccess) return fail(e, __LINE__);
     } else {
-        if ((e = cudaFuncSetAttribute(td_serve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) return fail(e, __LINE__);
-        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, td_serve_kernel<false>, warps * 32, smem)) != cudaSuccess) return fail(e, __LINE__);
+        if ((e = cudaFuncSetAttribute(td_serve_kernel<TD_SERVE_FREE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) return fail(e, __LINE__);
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, td_serve_kernel<TD_SERVE_FREE>, warps * 32, smem)) != cudaSuccess) return fail(e, __LINE__);
     }
     const int grid = g_dev[device].sms * std::max(1, per_sm);
     sv->workers = grid * warps - 1;
@@ -404,15 +426,15 @@ TD_API int td_serve_open(int device, unsigned ring_size, unsigned flags, double 
     }
     const uint64_t limit_ns = (uint64_t)((time_limit_s > 0 ? time_limit_s : 60.0) * 1e9);
     if (ordered)
-        td_serve_kernel<true><<<grid, warps * 32, smem, sv->stream>>>(
+        td_serve_kernel<TD_SERVE_ORDERED><<<grid, warps * 32, smem, sv->stream>>>(
             sv->d_ring, sv->d_res, sv->d_done, ring_size, sv->d_hctl, sv->d_ctl, sv->d_queue, sv->d_state,
             sv->d_pool, sv->d_items, sv->d_ready, sv->item_capacity, cfg.serve_grain, cfg.serve_split_level,
-            cfg.serve_check_every, 0, limit_ns, nullptr, 0);
+            cfg.serve_check_every, 0, limit_ns, nullptr, 0, 0u, 0ull);
     else
-        td_serve_kernel<false><<<grid, warps * 32, smem, sv->stream>>>(
+        td_serve_kernel<TD_SERVE_FREE><<<grid, warps * 32, smem, sv->stream>>>(
             sv->d_ring, sv->d_res, sv->d_done, ring_size, sv->d_hctl, sv->d_ctl, sv->d_queue, sv->d_state,
             sv->d_pool, sv->d_items, sv->d_ready, sv->item_capacity, cfg.serve_grain, cfg.serve_split_level,
-            cfg.serve_check_every, 0, limit_ns, sv->d_tt, tt_bits);
+            cfg.serve_check_every, 0, limit_ns, sv->d_tt, tt_bits, 0u, 0ull);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, __LINE__);
     *handle = sv;
     return TD_OK;

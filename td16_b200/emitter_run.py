@@ -9,11 +9,17 @@ witness, and hand the witnesses to the certificate sink in the reference's
 byte format (CertificateCodec).  Afterwards every stored record is read back
 and replayed on the GPU with the checker's rules.
 
-Batching is the one change to the reference's shape: a slot thread searches a
-batch of cases per call instead of one case per blocking call.
+Three shapes of the host side (--mode):
+  batch     a slot thread searches a batch of cases per call (td_search_batch)
+  percall   the reference's shape: one blocking td_search per case from
+            `slots` native threads, one per slot (GPUSortingSearch.java:134-162)
+  consumer  the enumerator's shape: generator threads hand cases one at a
+            time to a thread-safe consumer (DirectTwistedBraceletGenerator.
+            generateRepresentativesConcurrently), here host.PairBatcher, which
+            searches them in batches with td_search_pairs
 
-    python -m td16_b200.emitter_run [--count N] [--slots 16] [--budget-gib 4]
-                                    [--batch 65536] [--out certs.bin]
+    python -m td16_b200.emitter_run [--mode batch] [--count N] [--slots 16]
+                                    [--budget-gib 4] [--batch 65536] [--out certs.bin]
 """
 from __future__ import annotations
 
@@ -70,6 +76,106 @@ def replay_file(path: str, n_symbols: int, chunk: int = 1 << 20) -> dict:
     return {"records": total, "accepted": accepted, "replay_s": time.perf_counter() - t0}
 
 
+def _chunk(seed: int, k: int, c: int):
+    """Chunk k of the case stream: case j uses splitmix64 seeded with
+    (seed ^ k << 32) ^ j (near-reverse S_16)."""
+    perms, n = _lib.synth_perms(seed ^ (k << 32), c, 16, 16, 100, 1, 4)
+    return perms, n
+
+
+def _records(status, depth, moves):
+    """td_result records of per-call outcomes (status 1 found, else not)."""
+    res = np.zeros(len(status), _lib.RESULT_DTYPE)
+    res["status"] = np.where(status == 1, 1, 0)
+    res["depth"] = depth
+    m = moves.astype(np.uint16)
+    res["moves"] = m[:, :, 0] | (m[:, :, 1] << 5) | (m[:, :, 2] << 10)
+    return res
+
+
+def run_percall(count: int, slots: int, budget: int, out_path: str, seed: int = 4, device: int = 0,
+                chunk: int = 1 << 18) -> dict:
+    """One blocking td_search per case from `slots` native threads."""
+    _lib.init_slots(slots, [device], budget)
+    if os.path.exists(out_path):
+        os.remove(out_path)
+    writer = _lib.CertificateWriter(out_path, 5.0)
+    fn = _lib.entry_address("td_search")
+    found = not_found = errors = queued = 0
+    search_s = 0.0
+    t0 = time.perf_counter()
+    try:
+        for k in range((count + chunk - 1) // chunk):
+            c = min(chunk, count - k * chunk)
+            perms, n = _chunk(seed, k, c)
+            beta, omega = _pairs(perms, n)
+            init = (_lib.prepare_perms(perms, n, 9)["packed"] & 31).astype(np.int32)
+            r = _lib.slot_threads_run(fn, beta, omega, (n + 1).astype(np.int32), init, 0.0, 9, 1, slots)
+            search_s += r["seconds"]
+            found += int((r["status"] == 1).sum())
+            not_found += int((r["status"] == 0).sum())
+            errors += int((r["status"] < 0).sum())
+            res = _records(r["status"], r["depth"], r["moves"])
+            symbols = (n + 1).astype(np.uint8)
+            q = _lib.lib().td_cert_writer_enqueue_batch(writer._h, c, _lib._ptr(beta), _lib._ptr(omega),
+                                                        _lib._ptr(symbols), _lib._ptr(res))
+            if q < 0:
+                raise _lib.TdError(_lib.CUDA_ERROR, "certificate sink rejected a batch")
+            queued += int(q)
+    finally:
+        written = writer.close()
+        wall = time.perf_counter() - t0
+        _lib.destroy()
+    rep = replay_file(out_path, 17)
+    return {"mode": "percall", "cases": count, "slots": slots, "found": found, "not_found": not_found,
+            "errors": errors, "certificates": written, "wall_s": wall, "search_s": search_s,
+            "searches_per_s": count / search_s, "witnesses_per_s": written / wall, "replay": rep}
+
+
+def run_consumer(count: int, slots: int, budget: int, out_path: str, seed: int = 4, device: int = 0,
+                 generators: int = 8, batch: int = 8192) -> dict:
+    """Generator threads hand cases one at a time to host.PairBatcher."""
+    from .host import PairBatcher
+    _lib.init_slots(slots, [device], budget)
+    if os.path.exists(out_path):
+        os.remove(out_path)
+    writer = _lib.CertificateWriter(out_path, 5.0)
+    perms, n = _chunk(seed, 0, count)
+    beta, omega = _pairs(perms, n)
+    init = (_lib.prepare_perms(perms, n, 9)["packed"] & 31).astype(np.int32)
+    lock = threading.Lock()
+    sink_calls = [0]
+
+    def sink(b, o, witness):
+        writer.enqueue(o, witness)
+        with lock:
+            sink_calls[0] += 1
+
+    t0 = time.perf_counter()
+    batcher = PairBatcher(range(slots), batch_size=batch, max_delay_s=0.005, sink=sink)
+    futures = [None] * count
+
+    def generate(g):
+        for i in range(g, count, generators):
+            futures[i] = batcher.accept(beta[i, :17].tobytes(), omega[i, :17].tobytes(), int(init[i]), 0.0, 9)
+
+    threads = [threading.Thread(target=generate, args=(g,)) for g in range(generators)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    batcher.close()
+    results = [f.result() for f in futures]
+    written = writer.close()
+    wall = time.perf_counter() - t0
+    _lib.destroy()
+    rep = replay_file(out_path, 17)
+    return {"mode": "consumer", "cases": count, "slots": slots, "generators": generators, "batch": batch,
+            "batches": batcher.batches, "found": sum(bool(r) for r in results),
+            "not_found": sum(not r for r in results), "certificates": written, "wall_s": wall,
+            "witnesses_per_s": written / wall, "replay": rep}
+
+
 def run(count: int, slots: int, budget: int, batch: int, out_path: str, seed: int = 4, device: int = 0) -> dict:
     _lib.init_slots(slots, [device], budget)
     if os.path.exists(out_path):
@@ -89,8 +195,7 @@ def run(count: int, slots: int, budget: int, batch: int, out_path: str, seed: in
                 if k >= chunks:
                     return
                 c = min(batch, count - k * batch)
-                # chunk k, case j: splitmix64 seeded with (seed ^ k << 32) ^ j
-                perms, n = _lib.synth_perms(seed ^ (k << 32), c, 16, 16, 100, 1, 4)
+                perms, n = _chunk(seed, k, c)
                 inst = _lib.prepare_perms(perms, n, 9)
                 beta, omega = _pairs(perms, n)
                 res, st = _lib.search_batch(slot, inst, _lib.FLAG_VERIFY)
@@ -121,7 +226,7 @@ def run(count: int, slots: int, budget: int, batch: int, out_path: str, seed: in
         raise failure[0]
     rep = replay_file(out_path, 17)
     return {
-        "cases": count, "slots": slots, "budget_bytes": budget, "batch": batch,
+        "mode": "batch", "cases": count, "slots": slots, "budget_bytes": budget, "batch": batch,
         "found": state["found"], "not_found": state["not_found"], "errors": state["errors"],
         "certificates": written, "wall_s": wall, "witnesses_per_s": written / wall,
         "expansions": state["expansions"], "replay": rep,
@@ -136,8 +241,16 @@ def main():
     ap.add_argument("--batch", type=int, default=65536)
     ap.add_argument("--out", default="certs.bin")
     ap.add_argument("--seed", type=int, default=4)
+    ap.add_argument("--mode", default="batch", choices=["batch", "percall", "consumer"])
     a = ap.parse_args()
-    print(json.dumps(run(a.count, a.slots, int(a.budget_gib * (1 << 30)), a.batch, a.out, a.seed)))
+    budget = int(a.budget_gib * (1 << 30))
+    if a.mode == "percall":
+        out = run_percall(a.count, a.slots, budget, a.out, a.seed)
+    elif a.mode == "consumer":
+        out = run_consumer(a.count, a.slots, budget, a.out, a.seed)
+    else:
+        out = run(a.count, a.slots, budget, a.batch, a.out, a.seed)
+    print(json.dumps(out))
 
 
 if __name__ == "__main__":

@@ -272,3 +272,138 @@ class GPUSortingSearch:
         if not positions:
             return []
         return _lib.positions_to_symbols(beta, positions)
+
+
+class PairBatcher:
+    """A case consumer that searches pairs in batches.
+
+    The enumerator hands every canonical pair to a thread-safe
+    Consumer<CyclicTargetPair> from many generator threads
+    (DirectTwistedBraceletGenerator.generateRepresentativesConcurrently,
+    emitter/src/main/java/br/unb/cic/tdp/DirectTwistedBraceletGenerator.java:105-156),
+    and the consumer makes one blocking search per pair through the slot queue
+    (GPUSortingSearch.java:134-162).  This consumer collects the pairs instead:
+    a batch is handed to a slot worker when it holds `batch_size` pairs or
+    when its oldest pair has waited `max_delay_s`, and the worker searches it
+    with one td_search_pairs call.  `accept` returns a future of the witness
+    as symbol triples (a, b, c) on the pair's beta, [] when there is none; the
+    optional `sink(beta, omega, witness)` receives every found witness (e.g. a
+    certificate writer).  At most `max_pending` batches wait for a worker;
+    `accept` blocks beyond that, like the reference's bounded queue of
+    slots + tdp.gpuQueueCapacity jobs.  `search_fn` replaces the engine call
+    (the CPU tests use it)."""
+
+    def __init__(self, slots, batch_size: int = 4096, max_delay_s: float = 0.002, max_pending: int | None = None,
+                 sink=None, search_fn=None):
+        self.slots = list(slots)
+        if not self.slots or batch_size <= 0 or max_delay_s <= 0:
+            raise ValueError("a batcher needs slots, a positive batch size and a positive delay")
+        self.batch_size = int(batch_size)
+        self.max_delay_s = float(max_delay_s)
+        self.sink = sink
+        self._search = search_fn or _lib.search_pairs
+        self._cv = threading.Condition()
+        self._open: list = []          # (beta, omega, init, rate, maxd, full, future) of the filling batch
+        self._opened_at = 0.0
+        self._ready: list = []         # full or expired batches
+        self._max_pending = max_pending or 2 * len(self.slots)
+        self._closed = False
+        self.batches = 0
+        self.pairs = 0
+        self._threads = [threading.Thread(target=self._work, args=(s,), daemon=True, name=f"pair-batcher-slot-{s}")
+                         for s in self.slots]
+        self._timer = threading.Thread(target=self._tick, daemon=True, name="pair-batcher-timer")
+        for t in self._threads:
+            t.start()
+        self._timer.start()
+
+    def accept(self, beta, omega, initial_even_cycles: int, min_rate: float, max_moves: int,
+               full_sorting: bool = True) -> cf.Future:
+        fut: cf.Future = cf.Future()
+        beta, omega = bytes(beta), bytes(omega)
+        if len(beta) != len(omega):
+            fut.set_exception(_lib.TdError(_lib.INVALID_ARG, "beta and omega must have equal lengths"))
+            return fut
+        with self._cv:
+            if self._closed:
+                raise RuntimeError("the batcher is closed")
+            while len(self._ready) >= self._max_pending:
+                self._cv.wait()
+            if not self._open:
+                self._opened_at = time.monotonic()
+            self._open.append((beta, omega, int(initial_even_cycles), float(min_rate), int(max_moves),
+                               bool(full_sorting), fut))
+            if len(self._open) >= self.batch_size:
+                self._ready.append(self._open)
+                self._open = []
+                self._cv.notify_all()
+        return fut
+
+    def _tick(self):
+        with self._cv:
+            while not self._closed:
+                if self._open and time.monotonic() - self._opened_at >= self.max_delay_s:
+                    self._ready.append(self._open)
+                    self._open = []
+                    self._cv.notify_all()
+                self._cv.wait(timeout=self.max_delay_s / 2)
+
+    def _work(self, slot: int):
+        while True:
+            with self._cv:
+                while not self._ready and not self._closed:
+                    self._cv.wait()
+                if not self._ready:
+                    return
+                batch = self._ready.pop(0)
+                self._cv.notify_all()
+            self._run(slot, batch)
+
+    def _run(self, slot: int, batch):
+        c = len(batch)
+        beta = np.zeros((c, 17), np.uint8)
+        omega = np.zeros((c, 17), np.uint8)
+        n = np.zeros(c, np.uint8)
+        for i, p in enumerate(batch):
+            k = min(len(p[0]), 17)
+            beta[i, :k] = np.frombuffer(p[0][:k], np.uint8)
+            omega[i, :k] = np.frombuffer(p[1][:k], np.uint8)
+            n[i] = len(p[0]) if len(p[0]) <= 17 else 255
+        cols = [np.array([p[f] for p in batch], dt) for f, dt in ((2, np.int32), (3, np.float32), (4, np.int32),
+                                                                   (5, np.uint8))]
+        try:
+            status, depth, moves = self._search(slot, beta, omega, n, *cols)
+        except BaseException as e:  # noqa: BLE001 - delivered to every caller in the batch
+            for p in batch:
+                p[6].set_exception(e)
+            return
+        messages = {_lib.OVERFLOW: "GPU sorting search queue overflow",
+                    _lib.TIMEOUT: "GPU sorting search deadline reached",
+                    _lib.INVALID_ARG: "performGpuSortingSearch: invalid input"}
+        for i, p in enumerate(batch):
+            st = int(status[i])
+            if st == _lib.OK:
+                positions = [tuple(int(v) for v in moves[i, d]) for d in range(int(depth[i]))]
+                witness = _lib.positions_to_symbols(p[0], positions)
+                if self.sink is not None:
+                    self.sink(p[0], p[1], witness)
+                p[6].set_result(witness)
+            elif st == _lib.NOT_FOUND:
+                p[6].set_result([])
+            else:
+                p[6].set_exception(_lib.TdError(st, messages.get(st, "GPU sorting search failed")))
+        with self._cv:
+            self.batches += 1
+            self.pairs += c
+
+    def close(self) -> None:
+        """Searches what was accepted, then stops the workers."""
+        with self._cv:
+            if self._open:
+                self._ready.append(self._open)
+                self._open = []
+            self._closed = True
+            self._cv.notify_all()
+        for t in self._threads:
+            t.join()
+        self._timer.join()

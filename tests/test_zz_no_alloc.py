@@ -87,3 +87,26 @@ def test_noalloc_rejects_batches_beyond_its_scratch(td):
     d = torch.zeros(16, dtype=torch.uint8, device="cuda")
     rc, msg = _call(f, MAX_INSTANCES + 1, d, d, 0, 0)
     assert rc == 4 and "65536" in msg
+
+
+def test_noalloc_calls_leave_device_memory_unchanged(td):
+    """After the one-time set-up of the first call, calls take no device
+    memory: the device's free bytes are the same before and after two more
+    calls (nothing else allocates inside that window)."""
+    import torch
+    f = _noalloc(td)
+    perms, n = td.synth_perms(44, 8192, 13, 16, 50, 1, 3)
+    batch = td.prepare_perms(perms, n, (n // 2 + 1).astype(np.int32))
+    d_in = torch.from_numpy(batch.view(np.uint8).copy()).cuda()
+    d_out = torch.zeros(len(batch) * 32, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    rc, msg = _call(f, len(batch), d_in, d_out, td._lib.FLAG_VERIFY, stream)   # set-up call
+    assert rc == 0, msg
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    for flags in (td._lib.FLAG_VERIFY, td._lib.FLAG_ORDERED | td._lib.FLAG_PLAIN):
+        rc, msg = _call(f, len(batch), d_in, d_out, flags, stream)
+        assert rc == 0, msg
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before
