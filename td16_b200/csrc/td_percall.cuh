@@ -49,9 +49,12 @@ struct PercallServer {
     uint64_t *d_tt = nullptr;
     size_t tt_warps = 0;
     int tt_bits = 0;
+    // tickets are numbered across the launches of this server, so a stamp of
+    // one launch never matches a request of another
     unsigned long long published = 0;
     unsigned long long *taken = nullptr;  // per ring slot: ticket + 1 of the last result read
     int inflight = 0;
+    std::atomic<unsigned> generation{0};  // launches started; a waiting client compares it
     std::chrono::steady_clock::time_point started;
     int grid = 0;
 };
@@ -87,7 +90,26 @@ void percall_free(PercallServer &ps) {
     if (ps.d_tt) cudaFree(ps.d_tt);
     if (ps.stream) cudaStreamDestroy(ps.stream);
     delete[] ps.taken;
-    ps = PercallServer{};
+    ps.allocated = ps.running = ps.retiring = false;
+    ps.device = -1;
+    ps.stream = nullptr;
+    ps.h_ring = ps.d_ring = nullptr;
+    ps.h_res = ps.d_res = nullptr;
+    ps.h_done = ps.d_done = nullptr;
+    ps.h_ctl = ps.d_hctl = nullptr;
+    ps.d_ctl = nullptr;
+    ps.d_queue = nullptr;
+    ps.d_state = nullptr;
+    ps.d_pool = nullptr;
+    ps.d_items = nullptr;
+    ps.d_ready = nullptr;
+    ps.d_tt = nullptr;
+    ps.tt_warps = 0;
+    ps.tt_bits = 0;
+    ps.published = 0;
+    ps.taken = nullptr;
+    ps.inflight = 0;
+    ps.generation.fetch_add(1);
 }
 
 int percall_alloc(PercallServer &ps, int device, char *err, size_t errlen) {
@@ -117,6 +139,9 @@ int percall_alloc(PercallServer &ps, int device, char *err, size_t errlen) {
         return TD_CUDA_ERROR;
     }
     ps.taken = new unsigned long long[R];
+    std::memset(ps.taken, 0, sizeof(unsigned long long) * R);
+    std::memset((void *)ps.h_done, 0, sizeof(unsigned long long) * R);
+    ps.published = 0;
     return TD_OK;
 }
 
@@ -155,14 +180,15 @@ int percall_start(PercallServer &ps, int device, char *err, size_t errlen) {
         ps.tt_warps = (size_t)grid * warps;
         ps.tt_bits = cfg.tt_bits;
     }
-    // a fresh ticket sequence: clear the stamps, the taken marks and the
-    // item tags of the previous launch
-    std::memset((void *)ps.h_done, 0, sizeof(unsigned long long) * kPercallRing);
-    std::memset((void *)ps.h_ctl, 0, sizeof(td_serve_host_ctl));
-    std::memset(ps.taken, 0, sizeof(unsigned long long) * kPercallRing);
-    ps.published = 0;
-    ps.inflight = 0;
-    TD_CHECK(cudaMemsetAsync(ps.d_ctl, 0, sizeof(td_serve_dev_ctl), ps.stream));
+    // the launch starts at the next ticket: its dispatcher and workers begin
+    // there, and the item tags of the previous launch are cleared
+    td_serve_dev_ctl ctl;
+    std::memset(&ctl, 0, sizeof ctl);
+    ctl.available = ctl.claimed = ps.published;
+    ps.h_ctl->stop = 0;
+    __atomic_store_n(const_cast<unsigned long long *>(&ps.h_ctl->published), ps.published, __ATOMIC_RELEASE);
+    TD_CHECK(cudaMemcpyAsync(ps.d_ctl, &ctl, sizeof ctl, cudaMemcpyHostToDevice, ps.stream));
+    TD_CHECK(cudaStreamSynchronize(ps.stream));  // `ctl` lives on this stack
     TD_CHECK(cudaMemsetAsync(ps.d_pool, 0, sizeof(td_pool), ps.stream));
     TD_CHECK(cudaMemsetAsync(ps.d_ready, 0, sizeof(uint32_t) * kPercallItems, ps.stream));
     const uint64_t request_ns = time_limit_ns();
@@ -176,6 +202,7 @@ int percall_start(PercallServer &ps, int device, char *err, size_t errlen) {
     ps.running = true;
     ps.retiring = false;
     ps.started = std::chrono::steady_clock::now();
+    ps.generation.fetch_add(1);
     return TD_OK;
 }
 
@@ -211,6 +238,7 @@ int percall_search(int device, const td_instance &x, td_result *out, char *err, 
     PercallDevice &pd = g_percall[device];
     PercallServer *ps;
     unsigned long long ticket;
+    unsigned gen;
     {
         std::lock_guard<std::mutex> g(pd.mu);
         TD_CHECK(cudaSetDevice(device));
@@ -248,6 +276,7 @@ int percall_search(int device, const td_instance &x, td_result *out, char *err, 
         ps->published = ticket + 1;
         __atomic_store_n(const_cast<unsigned long long *>(&ps->h_ctl->published), ticket + 1, __ATOMIC_RELEASE);
         ++ps->inflight;
+        gen = ps->generation.load();
     }
     const unsigned slot = (unsigned)(ticket % kPercallRing);
     int rc = TD_OK;
@@ -257,7 +286,9 @@ int percall_search(int device, const td_instance &x, td_result *out, char *err, 
             break;
         }
         if ((spin & 1023u) == 0) {
-            const cudaError_t q = cudaStreamQuery(ps->stream);
+            // the launch this request went to has ended (its deadline, an
+            // error) or been replaced after it ended: the request is lost
+            const cudaError_t q = ps->generation.load() != gen ? cudaSuccess : cudaStreamQuery(ps->stream);
             if (q != cudaErrorNotReady) {
                 if (__atomic_load_n(&ps->h_done[slot], __ATOMIC_ACQUIRE) == ticket + 1) continue;
                 if (q == cudaSuccess) {

@@ -79,8 +79,9 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
     td_block_init(lut, ws, warps);
     const uint64_t deadline = td_globaltimer() + time_limit_ns;
     if (blockIdx.x == 0 && warp == 0) {
-        // dispatcher: host ring -> device queue
-        unsigned long long avail = 0;
+        // dispatcher: host ring -> device queue, from the launch's first
+        // ticket (0, or where the previous launch of a per-call server ended)
+        unsigned long long avail = *(volatile unsigned long long *)&dctl->available;
         unsigned backoff = 256;
         for (;;) {
             const int hstop = hctl->stop;
