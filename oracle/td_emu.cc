@@ -264,9 +264,10 @@ int next_child(Emu &e, int level, int *accepted) {
 }
 
 // The kernel's table of explored states (free order): 2^12 entries, key =
-// td_tt_key of the pinned state (nibbles from N-1 on cleared), a 3-bit
-// generation, the depth in the top nibble, direct-mapped by a multiplicative
-// hash.
+// td_tt_key of the pinned state (nibbles from N-1 on cleared) times an odd
+// constant modulo 2^57, the top 12 bits the slot and the rest the tag, a
+// 15-bit generation, the depth in the top nibble.  The generation counter
+// persists across searches on a thread, as the kernel's does across units.
 #define EMU_TT_BITS 12
 // restart budget base of the free order (the kernel's default); 0 = none
 static uint32_t g_restart_base = 16;
@@ -278,17 +279,28 @@ extern "C" uint32_t td_emu_budget(uint32_t base, int a) { return td_attempt_budg
 extern "C" int td_emu_restarts(void) { return TD_RESTARTS; }
 bool tt_visit(uint64_t *tt, uint64_t L, int N, int lv, uint32_t gen) {
     const uint64_t data = N - 1 >= 16 ? ~0ull : ((1ull << (4 * (N - 1))) - 1ull);
-    const uint64_t key = td_tt_key(L & data);
-    const uint64_t tag = key | ((uint64_t)gen << 57);
-    const unsigned h = (unsigned)((key * 0x9E3779B97F4A7C15ull) >> (64 - EMU_TT_BITS));
-    const uint64_t old = tt[h];
-    if ((old & (0x01ffffffffffffffull | (7ull << 57))) == tag && (int)(old >> 60) <= lv) return true;
-    tt[h] = tag | ((uint64_t)lv << 60);
+    const uint64_t h = (td_tt_key(L & data) * 0x9E3779B97F4A7C15ull) & 0x01ffffffffffffffull;
+    const int tag_bits = 57 - EMU_TT_BITS;
+    const unsigned slot = (unsigned)(h >> tag_bits);
+    const uint64_t want = (h & ((1ull << tag_bits) - 1ull)) | ((uint64_t)gen << tag_bits);
+    const uint64_t old = tt[slot];
+    if ((old & ((1ull << 60) - 1ull)) == want && (int)(old >> 60) <= lv) return true;
+    tt[slot] = want | ((uint64_t)lv << 60);
     return false;
 }
 
+// the next generation of the thread's table; clears it when the counter wraps
+uint32_t tt_next_gen(uint64_t *tt, uint32_t &counter) {
+    if (++counter >= (1u << (EMU_TT_BITS + 3))) {
+        for (int q = 0; q < (1 << EMU_TT_BITS); ++q) tt[q] = 0;
+        counter = 1;
+    }
+    return counter;
+}
+
 int search_rows(Emu &e, td_result *res) {
-    static thread_local uint64_t tt[1 << EMU_TT_BITS];
+    static thread_local uint64_t tt[1 << EMU_TT_BITS];  // zero-initialised: every word empty
+    static thread_local uint32_t tt_counter = 0;
     bool tt_on = false;  // in use after 32 expansions, as in the kernel
     uint32_t tt_gen = 0;
     int attempt = 0;     // restarts, as in the kernel
@@ -313,7 +325,7 @@ int search_rows(Emu &e, td_result *res) {
             ord = td_order_variant(attempt);
             attempt_budget = td_attempt_budget(g_restart_base, attempt);
             attempt_exp = 1;
-            if (tt_on && (tt_gen = (tt_gen + 1) % 8) == 0) tt_on = false;  // wrapped: clear
+            if (tt_on) tt_gen = tt_next_gen(tt, tt_counter);  // the abandoned attempt's entries no longer match
             level = 0;
             odd = prepare_rows(e, e.L[0], e.off[0]);
             found = evaluate_rows(e, 0, odd);
@@ -330,7 +342,7 @@ int search_rows(Emu &e, td_result *res) {
         td_apply_move(e.L[level], e.off[level], e.N, t & 31, (t >> 5) & 31, (t >> 10) & 31, &e.L[level + 1], &noff);
         e.off[level + 1] = noff;
         if (!tt_on && e.expansions >= 32) {
-            for (int q = 0; q < (1 << EMU_TT_BITS); ++q) tt[q] = ~0ull;
+            tt_gen = tt_next_gen(tt, tt_counter);
             tt_on = true;
         }
         if (tt_on && tt_visit(tt, e.L[level + 1], e.N, level + 1, tt_gen)) continue;  // explored with at least this budget

@@ -79,6 +79,7 @@ __device__ __forceinline__ td_search_limits td_make_limits(uint64_t max_exp, uin
     lim.deadline_ns = time_limit_ns ? td_globaltimer() + time_limit_ns : 0;
     lim.abort_flag = abort_flag;
     lim.tt = nullptr;
+    lim.tt_gen = nullptr;
     lim.tt_bits = 0;
     lim.restart_base = 0;
     return lim;
@@ -182,8 +183,9 @@ __global__ void __launch_bounds__(256, TD_STEAL_MIN_BLOCKS) td_steal_kernel(cons
                                                       td_item *items, uint32_t *ready, const uint32_t *epoch_ptr,
                                                       int capacity, td_inst_state *state, int grain,
                                                       int max_level, int check_every, uint64_t time_limit_ns,
-                                                      uint64_t *tt, int tt_bits, uint32_t restart_base,
-                                                      uint64_t max_exp, unsigned max_backoff_ns) {
+                                                      uint64_t *tt, uint32_t *tt_gen, int tt_bits,
+                                                      uint32_t restart_base, uint64_t max_exp,
+                                                      unsigned max_backoff_ns) {
     extern __shared__ __align__(16) uint8_t td_smem[];
     const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // free order only: no class table, the warp frames start the block's shared memory
@@ -200,6 +202,7 @@ __global__ void __launch_bounds__(256, TD_STEAL_MIN_BLOCKS) td_steal_kernel(cons
     lim.restart_base = restart_base;
     if (tt) {
         lim.tt = tt + ((size_t)(blockIdx.x * warps + warp) << tt_bits);
+        lim.tt_gen = tt_gen + blockIdx.x * warps + warp;
         lim.tt_bits = tt_bits;
     }
     td_donate_ctx dc;
@@ -482,6 +485,7 @@ struct Slot {
     uint32_t *d_ready = nullptr;
     int item_capacity = 0;
     uint64_t *d_tt = nullptr;  // tables of explored states, one per resident warp
+    uint32_t *d_tt_gen = nullptr;  // their generation counters
     size_t tt_warps = 0;
     int tt_bits = 0;
     td_inst_state *d_state = nullptr;
@@ -642,6 +646,7 @@ void release_slot(Slot &s) {
     if (s.d_items) cudaFree(s.d_items);
     if (s.d_ready) cudaFree(s.d_ready);
     if (s.d_tt) cudaFree(s.d_tt);
+    if (s.d_tt_gen) cudaFree(s.d_tt_gen);
     if (s.d_epoch) cudaFree(s.d_epoch);
     if (s.d_state) cudaFree(s.d_state);
     if (s.d_counts) cudaFree(s.d_counts);
@@ -714,9 +719,16 @@ int launch_batch(Slot &s, int count, const td_instance *d_in, td_result *d_out, 
             // graph; the launch waits for the previous one before replacing it
             TD_CHECK(cudaStreamSynchronize(stream));
             if (s.d_tt) TD_CHECK(cudaFree(s.d_tt));
+            if (s.d_tt_gen) TD_CHECK(cudaFree(s.d_tt_gen));
             s.d_tt = nullptr;
+            s.d_tt_gen = nullptr;
             s.tt_warps = 0;
-            TD_CHECK(cudaMalloc(&s.d_tt, ((size_t)resident * warps << cfg.tt_bits) * sizeof(uint64_t)));
+            const size_t tt_words = (size_t)resident * warps << cfg.tt_bits;
+            TD_CHECK(cudaMalloc(&s.d_tt, tt_words * sizeof(uint64_t)));
+            TD_CHECK(cudaMalloc(&s.d_tt_gen, (size_t)resident * warps * sizeof(uint32_t)));
+            // zero words are empty, and generations start at 1
+            TD_CHECK(cudaMemsetAsync(s.d_tt, 0, tt_words * sizeof(uint64_t), stream));
+            TD_CHECK(cudaMemsetAsync(s.d_tt_gen, 0, (size_t)resident * warps * sizeof(uint32_t), stream));
             s.tt_warps = (size_t)resident * warps;
             s.tt_bits = cfg.tt_bits;
         }
@@ -726,7 +738,7 @@ int launch_batch(Slot &s, int count, const td_instance *d_in, td_result *d_out, 
         td_steal_kernel<<<grid, threads, steal_smem_bytes(warps), stream>>>(
             d_in, d_out, count, s.d_pool, s.d_items, s.d_ready, s.d_epoch, s.item_capacity, s.d_state,
             cfg.steal_grain, cfg.split_level, cfg.check_every, time_limit_ns(), cfg.tt_bits > 0 ? s.d_tt : nullptr,
-            cfg.tt_bits, cfg.restart_base, max_exp, count == 1 ? 4096u : 32768u);
+            s.d_tt_gen, cfg.tt_bits, cfg.restart_base, max_exp, count == 1 ? 4096u : 32768u);
         TD_CHECK(cudaGetLastError());
         td_finalize_kernel<<<std::max(1, std::min((count + 255) / 256, 2 * cfg.sms)), 256, 0, stream>>>(
             s.d_pool, s.d_state, d_out, count);
@@ -1557,7 +1569,7 @@ TD_API int td_search_batch_noalloc(int count, const td_instance *d_instances, td
         const int grid = d.sms * std::max(1, d.steal_blocks);
         td_steal_kernel<<<grid, threads, steal_smem_bytes(warps), st>>>(
             d_instances, d_results, count, pool, items, ready, epoch, TD_NOALLOC_ITEMS, state, grain, split_level,
-            check_every, limit, nullptr, 0, restart_base, max_exp, count == 1 ? 4096u : 32768u);
+            check_every, limit, nullptr, nullptr, 0, restart_base, max_exp, count == 1 ? 4096u : 32768u);
         TD_CHECK_NA(cudaGetLastError());
         td_finalize_kernel<<<std::max(1, std::min((count + 255) / 256, 2 * d.sms)), 256, 0, st>>>(pool, state,
                                                                                                 d_results, count);

@@ -213,6 +213,7 @@ struct td_search_limits {
     uint64_t deadline_ns;      // %globaltimer value; 0 = none
     const int *abort_flag;     // optional host/device abort request
     uint64_t *tt;              // this warp's table of explored states (free order); null = none
+    uint32_t *tt_gen;          // this warp's generation counter of that table (kept across launches)
     int tt_bits;               // log2 of its entries
     uint32_t restart_base;     // free order: base of the restart budgets (td_attempt_budget); 0 = none
 };
@@ -726,27 +727,49 @@ __device__ __forceinline__ int td_donate(td_warp_smem &s, const td_donate_ctx &d
 // the earlier node was explored with at least as much budget, unless it is an
 // ancestor still being explored (which has more budget) or its children were
 // donated (then their takers explore them).  The search stops at the first
-// witness, so every completed entry is a state without one.  An entry is one
-// word: the state (td_tt_key, 57 bits), a 3-bit generation and the depth in
-// the top nibble.  A unit clears its table before first use, since the rate
-// masks and the bound belong to the instance.  A restart abandons the entries
-// (their subtrees were not all searched) by moving to the next generation;
-// the table is cleared again only when the generations wrap around.
+// witness, so every completed entry is a state without one.
+//
+// An entry is one word.  The state's 57-bit key (td_tt_key) is multiplied by
+// an odd constant modulo 2^57, a bijection; the top tt_bits bits of the
+// product pick the slot and the other 57 - tt_bits bits are stored as the
+// tag, so (slot, tag) still identifies the state.  That leaves tt_bits + 3
+// bits for a generation (15 at the default 4096 entries) under the depth in
+// the top nibble.  Entries of other generations never match.  Each unit that
+// uses the table, and each restart (which abandons the entries of the
+// attempt: their subtrees were not all searched), takes the warp's next
+// generation from a counter kept in global memory across units and launches,
+// so the table is cleared only when that counter wraps (every 32767 units at
+// 4096 entries) instead of once per unit.  Zero words are empty (generation 0
+// is never used).
 
-#define TD_TT_EMPTY 0xffffffffffffffffull  // no state has fifteen nibbles of 15
 // A unit starts using its table after this many expansions: most searches of
-// uniform permutations end sooner, and then clearing the table would cost
-// more than it saves.  States expanded before are simply not recorded.
+// uniform permutations end sooner, and they then never touch the table.
+// States expanded before are simply not recorded.
 #define TD_TT_AFTER 32
-#define TD_TT_KEY 0x01ffffffffffffffull  // bits 0-56 of an entry: the state
-#define TD_TT_GENS 8                       // generations per clear (bits 57-59)
+#define TD_TT_KEY 0x01ffffffffffffffull  // the 57 bits of a state key
+#define TD_TT_MULT 0x9E3779B97F4A7C15ull  // odd: multiplying by it permutes keys modulo 2^57
 
 __device__ __forceinline__ void td_tt_clear(const td_search_limits &lim) {
     const int lane = threadIdx.x & 31;
     uint4 *t = reinterpret_cast<uint4 *>(lim.tt);
     const int n4 = 1 << (lim.tt_bits - 1);
-    for (int q = lane; q < n4; q += 32) t[q] = make_uint4(~0u, ~0u, ~0u, ~0u);
+    for (int q = lane; q < n4; q += 32) t[q] = make_uint4(0u, 0u, 0u, 0u);
     __syncwarp();
+}
+
+// The warp's next table generation (uniform across the warp); clears the
+// table when the counter wraps.
+__device__ __forceinline__ uint32_t td_tt_next_gen(const td_search_limits &lim) {
+    const uint32_t gmax = (1u << (lim.tt_bits + 3)) - 1u;
+    uint32_t g = *(volatile uint32_t *)lim.tt_gen + 1u;
+    __syncwarp();
+    if (g > gmax) {
+        td_tt_clear(lim);
+        g = 1u;
+    }
+    if ((threadIdx.x & 31) == 0) *lim.tt_gen = g;
+    __syncwarp();
+    return g;
 }
 
 // Looks up the state of level `lv` (depth lv) in generation `gen` of the table
@@ -768,14 +791,15 @@ __device__ __forceinline__ bool td_tt_visit(const td_warp_smem &s, const td_sear
     }
     lo = __reduce_or_sync(TD_FULL, lo);
     hi = __reduce_or_sync(TD_FULL, hi);
-    const uint64_t key = td_tt_key((((uint64_t)hi) << 32) | lo);
-    const uint64_t tag = key | ((uint64_t)gen << 57);
     int hit = 0;
     if (m == 0) {
-        const uint32_t h = (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> (64 - lim.tt_bits));
-        const uint64_t old = lim.tt[h];
-        hit = (old & (TD_TT_KEY | (7ull << 57))) == tag && (int)(old >> 60) <= lv;
-        if (!hit) lim.tt[h] = tag | ((uint64_t)lv << 60);
+        const uint64_t h = (td_tt_key((((uint64_t)hi) << 32) | lo) * TD_TT_MULT) & TD_TT_KEY;
+        const int tag_bits = 57 - lim.tt_bits;
+        const uint32_t slot = (uint32_t)(h >> tag_bits);
+        const uint64_t want = (h & ((1ull << tag_bits) - 1ull)) | ((uint64_t)gen << tag_bits);
+        const uint64_t old = lim.tt[slot];
+        hit = (old & ((1ull << 60) - 1ull)) == want && (int)(old >> 60) <= lv;
+        if (!hit) lim.tt[slot] = want | ((uint64_t)lv << 60);
     }
     return __shfl_sync(TD_FULL, hit, 0) != 0;
 }
@@ -836,7 +860,7 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
                 ord = td_order_variant(attempt);
                 attempt_budget = td_attempt_budget(lim.restart_base, attempt);
                 attempt_exp = 1;
-                if (tt_on && (tt_gen = (tt_gen + 1) % TD_TT_GENS) == 0) tt_on = false;  // wrapped: clear
+                if (tt_on) tt_gen = td_tt_next_gen(lim);  // the abandoned attempt's entries no longer match
                 level = d0;
                 const int odd = td_prepare_rows(s, d0, N, O, F);
                 found = td_evaluate_rows(s, code, N, d0, odd, O, F);
@@ -909,7 +933,7 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
                 td_apply_bytes(s, level, t, N);
                 if (lim.tt) {
                     if (!tt_on && r.expansions >= TD_TT_AFTER) {
-                        td_tt_clear(lim);
+                        tt_gen = td_tt_next_gen(lim);
                         tt_on = true;
                     }
                     if (tt_on && td_tt_visit(s, lim, level + 1, N, tt_gen)) continue;  // explored with at least this budget

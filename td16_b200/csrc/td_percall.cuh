@@ -47,6 +47,7 @@ struct PercallServer {
     td_item *d_items = nullptr;
     uint32_t *d_ready = nullptr;
     uint64_t *d_tt = nullptr;
+    uint32_t *d_tt_gen = nullptr;
     size_t tt_warps = 0;
     int tt_bits = 0;
     // tickets are numbered across the launches of this server, so a stamp of
@@ -88,6 +89,7 @@ void percall_free(PercallServer &ps) {
     if (ps.d_items) cudaFree(ps.d_items);
     if (ps.d_ready) cudaFree(ps.d_ready);
     if (ps.d_tt) cudaFree(ps.d_tt);
+    if (ps.d_tt_gen) cudaFree(ps.d_tt_gen);
     if (ps.stream) cudaStreamDestroy(ps.stream);
     delete[] ps.taken;
     ps.allocated = ps.running = ps.retiring = false;
@@ -104,6 +106,7 @@ void percall_free(PercallServer &ps) {
     ps.d_items = nullptr;
     ps.d_ready = nullptr;
     ps.d_tt = nullptr;
+    ps.d_tt_gen = nullptr;
     ps.tt_warps = 0;
     ps.tt_bits = 0;
     ps.published = 0;
@@ -174,9 +177,15 @@ int percall_start(PercallServer &ps, int device, char *err, size_t errlen) {
     const int grid = cfg.sms * std::max(1, per_sm / 2);
     if (cfg.tt_bits > 0 && ((size_t)grid * warps > ps.tt_warps || cfg.tt_bits != ps.tt_bits)) {
         if (ps.d_tt) TD_CHECK(cudaFree(ps.d_tt));
+        if (ps.d_tt_gen) TD_CHECK(cudaFree(ps.d_tt_gen));
         ps.d_tt = nullptr;
+        ps.d_tt_gen = nullptr;
         ps.tt_warps = 0;
-        TD_CHECK(cudaMalloc(&ps.d_tt, ((size_t)grid * warps << cfg.tt_bits) * sizeof(uint64_t)));
+        const size_t words = (size_t)grid * warps << cfg.tt_bits;
+        TD_CHECK(cudaMalloc(&ps.d_tt, words * sizeof(uint64_t)));
+        TD_CHECK(cudaMalloc(&ps.d_tt_gen, (size_t)grid * warps * sizeof(uint32_t)));
+        TD_CHECK(cudaMemsetAsync(ps.d_tt, 0, words * sizeof(uint64_t), ps.stream));
+        TD_CHECK(cudaMemsetAsync(ps.d_tt_gen, 0, (size_t)grid * warps * sizeof(uint32_t), ps.stream));
         ps.tt_warps = (size_t)grid * warps;
         ps.tt_bits = cfg.tt_bits;
     }
@@ -196,7 +205,7 @@ int percall_start(PercallServer &ps, int device, char *err, size_t errlen) {
     td_serve_kernel<TD_SERVE_PER_REQUEST><<<grid, warps * 32, smem, ps.stream>>>(
         ps.d_ring, ps.d_res, ps.d_done, kPercallRing, ps.d_hctl, ps.d_ctl, ps.d_queue, ps.d_state, ps.d_pool,
         ps.d_items, ps.d_ready, kPercallItems, cfg.serve_grain, cfg.serve_split_level, cfg.serve_check_every, 0,
-        life_ns, cfg.tt_bits > 0 ? ps.d_tt : nullptr, cfg.tt_bits, cfg.restart_base, request_ns);
+        life_ns, cfg.tt_bits > 0 ? ps.d_tt : nullptr, ps.d_tt_gen, cfg.tt_bits, cfg.restart_base, request_ns);
     TD_CHECK(cudaGetLastError());
     ps.grid = grid;
     ps.running = true;

@@ -69,8 +69,9 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
                                                       td_instance *queue, td_inst_state *state, td_pool *pool,
                                                       td_item *items, uint32_t *ready, int item_capacity,
                                                       int grain, int max_level, int check_every, uint64_t max_exp,
-                                                      uint64_t time_limit_ns, uint64_t *tt, int tt_bits,
-                                                      uint32_t restart_base, uint64_t request_limit_ns) {
+                                                      uint64_t time_limit_ns, uint64_t *tt, uint32_t *tt_gen,
+                                                      int tt_bits, uint32_t restart_base,
+                                                      uint64_t request_limit_ns) {
     constexpr bool ALL_ORDERED = MODE == TD_SERVE_ORDERED;
     extern __shared__ __align__(16) uint8_t td_smem[];
     const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -122,6 +123,7 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
     lim.deadline_ns = deadline;
     lim.abort_flag = nullptr;
     lim.tt = (!ALL_ORDERED && tt) ? tt + ((size_t)(blockIdx.x * warps + warp) << tt_bits) : nullptr;
+    lim.tt_gen = lim.tt ? tt_gen + blockIdx.x * warps + warp : nullptr;
     lim.tt_bits = tt_bits;
     lim.restart_base = 0;  // serving searches are not restarted
     td_donate_ctx dc;
@@ -319,6 +321,7 @@ struct Server {
     uint32_t *d_ready = nullptr;
     int item_capacity = 0;
     uint64_t *d_tt = nullptr;  // tables of explored states, one per worker warp (free order)
+    uint32_t *d_tt_gen = nullptr;  // their generation counters
     unsigned long long published = 0;
     int workers = 0;
     // per slot: ticket + 1 of the last request whose result the client took
@@ -342,6 +345,7 @@ void server_free(Server *sv) {
     if (sv->d_items) cudaFree(sv->d_items);
     if (sv->d_ready) cudaFree(sv->d_ready);
     if (sv->d_tt) cudaFree(sv->d_tt);
+    if (sv->d_tt_gen) cudaFree(sv->d_tt_gen);
     if (sv->stream) cudaStreamDestroy(sv->stream);
     delete sv;
 }
@@ -424,18 +428,24 @@ TD_API int td_serve_open(int device, unsigned ring_size, unsigned flags, double 
     if (tt_bits > 0) {
         const size_t tt_bytes = ((size_t)grid * warps << tt_bits) * sizeof(uint64_t);
         if ((e = cudaMalloc(&sv->d_tt, tt_bytes)) != cudaSuccess) return fail(e, __LINE__);
+        if ((e = cudaMalloc(&sv->d_tt_gen, (size_t)grid * warps * sizeof(uint32_t))) != cudaSuccess)
+            return fail(e, __LINE__);
+        if ((e = cudaMemsetAsync(sv->d_tt, 0, tt_bytes, sv->stream)) != cudaSuccess) return fail(e, __LINE__);
+        if ((e = cudaMemsetAsync(sv->d_tt_gen, 0, (size_t)grid * warps * sizeof(uint32_t), sv->stream)) !=
+            cudaSuccess)
+            return fail(e, __LINE__);
     }
     const uint64_t limit_ns = (uint64_t)((time_limit_s > 0 ? time_limit_s : 60.0) * 1e9);
     if (ordered)
         td_serve_kernel<TD_SERVE_ORDERED><<<grid, warps * 32, smem, sv->stream>>>(
             sv->d_ring, sv->d_res, sv->d_done, ring_size, sv->d_hctl, sv->d_ctl, sv->d_queue, sv->d_state,
             sv->d_pool, sv->d_items, sv->d_ready, sv->item_capacity, cfg.serve_grain, cfg.serve_split_level,
-            cfg.serve_check_every, 0, limit_ns, nullptr, 0, 0u, 0ull);
+            cfg.serve_check_every, 0, limit_ns, nullptr, nullptr, 0, 0u, 0ull);
     else
         td_serve_kernel<TD_SERVE_FREE><<<grid, warps * 32, smem, sv->stream>>>(
             sv->d_ring, sv->d_res, sv->d_done, ring_size, sv->d_hctl, sv->d_ctl, sv->d_queue, sv->d_state,
             sv->d_pool, sv->d_items, sv->d_ready, sv->item_capacity, cfg.serve_grain, cfg.serve_split_level,
-            cfg.serve_check_every, 0, limit_ns, sv->d_tt, tt_bits, 0u, 0ull);
+            cfg.serve_check_every, 0, limit_ns, sv->d_tt, sv->d_tt_gen, tt_bits, 0u, 0ull);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, __LINE__);
     *handle = sv;
     return TD_OK;
