@@ -236,6 +236,57 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def serving_legs(td, device):
+    """Serving (continuous batching), n uniform 8..16, bound floor(n/2)+1,
+    open-loop Poisson arrivals:
+      ring     the serving launch fed by one host producer through a mapped
+               ring (td_serve_open_loop), one host thread polling all results;
+      clients  the per-call server under one client thread per host core
+               (at most 16), each polling only its own requests
+               (td_percall_open_loop).
+    Both are swept up to saturation, then run at 80% of the saturated rate.
+    Admission: a request waits for a free client (or worker warp); the 64 GiB
+    frame pool of the ring form never binds, since a request's DFS frames live
+    in shared memory and its device state is 48 bytes."""
+    from td16_b200 import _lib
+    perms_s, n_s = td.synth_perms(3, 400000, 8, 16, 0, 0, 0)
+    inst_s = td.prepare_perms(perms_s, n_s, (n_s // 2 + 1).astype(np.int32))
+    keys = ("p50_ms", "p99_ms", "p999_ms", "served_per_s", "offered_per_s", "served", "admission_wait_ms_mean")
+    out = {"workload": "open-loop Poisson, n uniform 8..16, bound floor(n/2)+1",
+           "admission": "in-flight requests <= worker warps (ring) or client threads (clients); the 64 GiB frame "
+                        "pool never binds (frames live in shared memory)"}
+    def sweep(run, rates):
+        res, capacity = {}, 0.0
+        for rate in rates:
+            k = int(min(len(inst_s), max(10000, rate * 0.5)))
+            try:
+                _, sst = run(inst_s[:k], rate)
+            except _lib.TdError as e:
+                res[f"{int(rate)}_per_s"] = {"error": str(e)}
+                continue
+            res[f"{int(rate)}_per_s"] = {key: sst[key] for key in keys}
+            capacity = max(capacity, sst["served_per_s"])
+        if capacity > 0:
+            at80 = 0.8 * capacity
+            _, sst = run(inst_s[: int(min(len(inst_s), max(10000, at80 * 0.5)))], at80)
+            res["at_80pct_of_saturation"] = {key: sst[key] for key in keys}
+        res["saturated_per_s"] = capacity
+        return res
+
+    rates = (5000.0, 50000.0, 200000.0, 1000000.0, 2000000.0, 4000000.0)
+    out["ring"] = sweep(lambda x, r: _lib.serve_open_loop(device, x, r, seed=3), rates)
+    clients = max(1, min(16, os.cpu_count() or 1))
+    td.init_slots(1, [device], 64 << 20)
+    try:
+        out[f"clients_{clients}"] = sweep(lambda x, r: _lib.percall_open_loop(device, x, r, clients=clients, seed=5),
+                                          rates[:5])
+        _, bst = td.search_batch(0, inst_s[:100000], 0)
+        out["batched_per_s"] = 100000 / (bst.kernel_ms / 1e3)
+    finally:
+        td.destroy()
+    return out
+
+
 REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libtd16ref.so")
 
 
@@ -449,18 +500,7 @@ def run_engine(args):
     graph.close()
     serving = None
     if world == 1 and not only_engine:
-        perms_s, n_s = td.synth_perms(3, 100000, 8, 16, 0, 0, 0)
-        inst_s = td.prepare_perms(perms_s, n_s, (n_s // 2 + 1).astype(np.int32))
-        serving = {"workload": "open-loop Poisson, n uniform 8..16, bound floor(n/2)+1, 64 GiB frame pool"}
-        for rate in (5000.0, 50000.0, 200000.0):
-            try:
-                _, sst = _lib.serve_open_loop(local, inst_s[: int(min(100000, rate * 2))], rate, seed=3)
-                serving[f"{int(rate)}_per_s"] = {k: sst[k] for k in ("p50_ms", "p99_ms", "p999_ms", "served_per_s",
-                                                                     "offered_per_s", "served")}
-            except _lib.TdError as e:
-                serving[f"{int(rate)}_per_s"] = {"error": str(e)}
-        _, bst = td.search_batch(0, inst_s, 0)
-        serving["batched_per_s"] = len(inst_s) / (bst.kernel_ms / 1e3)
+        serving = serving_legs(td, local)
     cpu = cpu_baseline() if world == 1 and not only_engine else None
     percall = per_call_legs(td) if world == 1 and not only_engine else None
     line = {

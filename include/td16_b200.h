@@ -112,11 +112,15 @@ int td_search_ordered(int slot, const uint8_t *beta, const uint8_t *omega, int n
  * launch per device; the calling thread writes its request into pinned,
  * device-mapped memory and polls for the result, so a search costs no CUDA
  * API call.  The launch holds half of each SM's block slots while per-call
- * searches run; batch entry points stop it first when none is in flight.
- * mode 0: one launch per call on the slot's stream.  rotate_after_s > 0 sets
- * the age at which a server launch is replaced by a fresh one (default 300;
- * every wait of a launch is bounded by its deadline); 0 keeps the setting. */
-int td_configure_percall(int mode, double rotate_after_s);
+ * searches run; batch entry points stop it first when none is in flight, and
+ * it exits by itself once it has had no request for idle_exit_s and has no
+ * work left (default 0.005 s), so a device-wide synchronisation elsewhere
+ * (cudaDeviceSynchronize, cudaFree) waits for it at most that long after the
+ * last per-call search.  mode 0: one launch per call on the slot's stream.
+ * rotate_after_s > 0 sets the age at which a busy server launch is replaced
+ * by a fresh one (default 300; every wait of a launch is bounded by its
+ * deadline).  A value of 0 keeps that setting. */
+int td_configure_percall(int mode, double rotate_after_s, double idle_exit_s);
 
 int td_slot_count(void);
 int td_slot_device(int slot);           /* -1 for an invalid slot */
@@ -283,6 +287,16 @@ int td_serve_open_loop(int device, const td_instance *instances, int count,
                        double rate, uint64_t seed, uint64_t pool_bytes,
                        unsigned flags, td_result *results, td_serve_stats *stats,
                        char *err, size_t errlen);
+
+/* Open-loop Poisson stream of `count` requests at `rate` per second through
+ * the per-call server (no counterpart in the reference): `clients` host
+ * threads each wait for their requests' arrival times, submit them as
+ * td_search does and poll only their own tickets, so the latency (arrival to
+ * result in the client) includes any wait for a free client.  Admission is by
+ * client count.  Results land in results[i]. */
+int td_percall_open_loop(int device, const td_instance *instances, int count, double rate,
+                         uint64_t seed, int clients, td_result *results, td_serve_stats *stats,
+                         char *err, size_t errlen);
 
 /* ---- certificates (emitter/src/main/java/br/unb/cic/tdp/base/CertificateCodec.java) */
 

@@ -57,7 +57,7 @@ EXPORTS = ["td_init_slots", "td_search", "td_search_ordered", "td_slot_count", "
            "td_codec_key", "td_codec_value", "td_codec_decode_key", "td_codec_decode_value",
            "td_replay_symbols_device", "td_cert_writer_open", "td_cert_writer_enqueue", "td_cert_writer_close",
            "td_serve_open", "td_serve_workers", "td_serve_submit", "td_serve_poll", "td_serve_close",
-           "td_serve_open_loop", "td_configure_percall", "td_search_pairs", "td_cert_writer_enqueue_batch", "td_cert_read_file", "td_pairs_from_perms", "td_batch_graph_create", "td_batch_graph_launch", "td_batch_graph_destroy"]
+           "td_serve_open_loop", "td_configure_percall", "td_search_pairs", "td_percall_open_loop", "td_cert_writer_enqueue_batch", "td_cert_read_file", "td_pairs_from_perms", "td_batch_graph_create", "td_batch_graph_launch", "td_batch_graph_destroy"]
 
 
 def lib():
@@ -93,7 +93,9 @@ def lib():
     L.td_configure_table.argtypes = [C.c_int]
     L.td_configure_restart.argtypes = [C.c_int]
     L.td_set_time_limit.argtypes = [C.c_double]
-    L.td_configure_percall.argtypes = [C.c_int, C.c_double]
+    L.td_configure_percall.argtypes = [C.c_int, C.c_double, C.c_double]
+    L.td_percall_open_loop.argtypes = [C.c_int, vp, C.c_int, C.c_double, C.c_uint64, C.c_int, vp,
+                                       C.POINTER(ServeStats), cp, sz]
     L.td_search_pairs.argtypes = [C.c_int, C.c_int] + [vp] * 7 + [C.c_uint] + [vp] * 3 + [cp, sz]
     L.td_codec_key.argtypes = [vp, C.c_int, vp, C.c_int]
     L.td_codec_value.argtypes = [vp, C.c_int, vp, C.c_int]
@@ -299,11 +301,12 @@ def configure_restart(base: int) -> None:
         raise TdError(INVALID_ARG, "restart base must be 0 or >= 16")
 
 
-def configure_percall(mode: int, rotate_after_s: float = 0.0) -> None:
+def configure_percall(mode: int, rotate_after_s: float = 0.0, idle_exit_s: float = 0.0) -> None:
     """Per-call searches: 1 through the device's resident server (default),
-    0 one launch per call; rotate_after_s > 0 sets the server's rotation age."""
-    if lib().td_configure_percall(int(mode), float(rotate_after_s)) != OK:
-        raise TdError(INVALID_ARG, "per-call mode must be 0 or 1 and the rotation age >= 0")
+    0 one launch per call; rotate_after_s > 0 sets the server's rotation age,
+    idle_exit_s > 0 the idle time after which it exits by itself."""
+    if lib().td_configure_percall(int(mode), float(rotate_after_s), float(idle_exit_s)) != OK:
+        raise TdError(INVALID_ARG, "per-call mode must be 0 or 1 and the times >= 0")
 
 
 def configure_serve(grain: int, split_level: int, check_every: int) -> None:
@@ -429,6 +432,20 @@ def serve_open_loop(device: int, instances: np.ndarray, rate: float, seed: int =
     err = C.create_string_buffer(512)
     rc = lib().td_serve_open_loop(int(device), _ptr(instances), len(instances), float(rate), C.c_uint64(seed),
                                   C.c_uint64(pool_bytes), int(flags), _ptr(results), C.byref(st), err, 512)
+    check(rc, err)
+    return results, st.as_dict()
+
+
+def percall_open_loop(device: int, instances: np.ndarray, rate: float, clients: int = 64, seed: int = 3):
+    """Open-loop Poisson stream through the per-call server, latency measured
+    by client threads that poll only their own requests; returns (results,
+    stats dict)."""
+    instances = np.ascontiguousarray(instances, INSTANCE_DTYPE)
+    results = np.zeros(len(instances), RESULT_DTYPE)
+    st = ServeStats()
+    err = C.create_string_buffer(512)
+    rc = lib().td_percall_open_loop(int(device), _ptr(instances), len(instances), float(rate), C.c_uint64(seed),
+                                    int(clients), _ptr(results), C.byref(st), err, 512)
     check(rc, err)
     return results, st.as_dict()
 

@@ -696,16 +696,18 @@ int launch_batch(Slot &s, int count, const td_instance *d_in, td_result *d_out, 
             const size_t cap = std::max<size_t>(1024, std::min<size_t>(s.budget / 36, 1u << 26));
             TD_CHECK(cudaMalloc(&s.d_items, cap * sizeof(td_item)));
             TD_CHECK(cudaMalloc(&s.d_ready, cap * sizeof(uint32_t)));
-            TD_CHECK(cudaMemset(s.d_ready, 0, cap * sizeof(uint32_t)));
+            TD_CHECK(cudaMemsetAsync(s.d_ready, 0, cap * sizeof(uint32_t), stream));
             TD_CHECK(cudaMalloc(&s.d_epoch, sizeof(uint32_t)));
-            TD_CHECK(cudaMemset(s.d_epoch, 0, sizeof(uint32_t)));
+            TD_CHECK(cudaMemsetAsync(s.d_epoch, 0, sizeof(uint32_t), stream));
             s.item_capacity = (int)cap;
         }
+        // buffers grow in stream order: a cudaFree would wait for all work on
+        // the device, the per-call server's resident launch included
         if ((size_t)count > s.state_count) {
-            if (s.d_state) TD_CHECK(cudaFree(s.d_state));
+            if (s.d_state) TD_CHECK(cudaFreeAsync(s.d_state, stream));
             s.d_state = nullptr;
             s.state_count = 0;
-            TD_CHECK(cudaMalloc(&s.d_state, (size_t)count * sizeof(td_inst_state)));
+            TD_CHECK(cudaMallocAsync(&s.d_state, (size_t)count * sizeof(td_inst_state), stream));
             s.state_count = (size_t)count;
         }
         // at least the slot's share of the resident grid, so that a small batch
@@ -716,16 +718,15 @@ int launch_batch(Slot &s, int count, const td_instance *d_in, td_result *d_out, 
         if (cfg.tt_bits > 0 && ((size_t)resident * warps > s.tt_warps || cfg.tt_bits != s.tt_bits)) {
             // one table (8 bytes x 2^tt_bits) per resident warp, sized for
             // the whole resident grid so that it never moves under a captured
-            // graph; the launch waits for the previous one before replacing it
-            TD_CHECK(cudaStreamSynchronize(stream));
-            if (s.d_tt) TD_CHECK(cudaFree(s.d_tt));
-            if (s.d_tt_gen) TD_CHECK(cudaFree(s.d_tt_gen));
+            // graph; replaced in stream order after the previous launch
+            if (s.d_tt) TD_CHECK(cudaFreeAsync(s.d_tt, stream));
+            if (s.d_tt_gen) TD_CHECK(cudaFreeAsync(s.d_tt_gen, stream));
             s.d_tt = nullptr;
             s.d_tt_gen = nullptr;
             s.tt_warps = 0;
             const size_t tt_words = (size_t)resident * warps << cfg.tt_bits;
-            TD_CHECK(cudaMalloc(&s.d_tt, tt_words * sizeof(uint64_t)));
-            TD_CHECK(cudaMalloc(&s.d_tt_gen, (size_t)resident * warps * sizeof(uint32_t)));
+            TD_CHECK(cudaMallocAsync(&s.d_tt, tt_words * sizeof(uint64_t), stream));
+            TD_CHECK(cudaMallocAsync(&s.d_tt_gen, (size_t)resident * warps * sizeof(uint32_t), stream));
             // zero words are empty, and generations start at 1
             TD_CHECK(cudaMemsetAsync(s.d_tt, 0, tt_words * sizeof(uint64_t), stream));
             TD_CHECK(cudaMemsetAsync(s.d_tt_gen, 0, (size_t)resident * warps * sizeof(uint32_t), stream));
@@ -1185,11 +1186,11 @@ TD_API int td_search_batch(int slot, int count, const td_instance *in, td_result
     std::lock_guard<std::mutex> g(*s->mu);
     TD_CHECK(cudaSetDevice(s->device));
     const size_t need = (size_t)count * (sizeof(td_instance) + sizeof(td_result));
-    if (need > s->d_batch_bytes) {
-        if (s->d_batch) TD_CHECK(cudaFree(s->d_batch));
+    if (need > s->d_batch_bytes) {  // grows in stream order (no device-wide wait)
+        if (s->d_batch) TD_CHECK(cudaFreeAsync(s->d_batch, s->stream));
         s->d_batch = nullptr;
         s->d_batch_bytes = 0;
-        TD_CHECK(cudaMalloc(&s->d_batch, need));
+        TD_CHECK(cudaMallocAsync(&s->d_batch, need, s->stream));
         s->d_batch_bytes = need;
     }
     if (stats && !s->d_counts) TD_CHECK(cudaMalloc(&s->d_counts, sizeof(td_counts)));

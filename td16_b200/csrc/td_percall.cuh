@@ -57,7 +57,7 @@ struct PercallServer {
     int inflight = 0;
     std::atomic<unsigned> generation{0};  // launches started; a waiting client compares it
     std::chrono::steady_clock::time_point started;
-    int grid = 0;
+    int grid = 0, warps = 0;
 };
 
 struct PercallDevice {
@@ -69,6 +69,7 @@ struct PercallDevice {
 PercallDevice g_percall[kPercallDevices];
 std::atomic<int> g_percall_mode{1};  // 1: resident server, 0: one launch per call
 std::atomic<long long> g_percall_rotate_ns{300000000000ll};
+std::atomic<long long> g_percall_idle_ns{5000000ll};  // a launch idle this long exits by itself
 
 // rotation age of a launch; its deadline leaves every accepted request the
 // full search time limit on top
@@ -176,14 +177,16 @@ int percall_start(PercallServer &ps, int device, char *err, size_t errlen) {
     // half of each SM's block slots: batch launches keep the other half
     const int grid = cfg.sms * std::max(1, per_sm / 2);
     if (cfg.tt_bits > 0 && ((size_t)grid * warps > ps.tt_warps || cfg.tt_bits != ps.tt_bits)) {
-        if (ps.d_tt) TD_CHECK(cudaFree(ps.d_tt));
-        if (ps.d_tt_gen) TD_CHECK(cudaFree(ps.d_tt_gen));
+        // in stream order: a cudaFree would wait for the device's other
+        // server launch, which may be draining
+        if (ps.d_tt) TD_CHECK(cudaFreeAsync(ps.d_tt, ps.stream));
+        if (ps.d_tt_gen) TD_CHECK(cudaFreeAsync(ps.d_tt_gen, ps.stream));
         ps.d_tt = nullptr;
         ps.d_tt_gen = nullptr;
         ps.tt_warps = 0;
         const size_t words = (size_t)grid * warps << cfg.tt_bits;
-        TD_CHECK(cudaMalloc(&ps.d_tt, words * sizeof(uint64_t)));
-        TD_CHECK(cudaMalloc(&ps.d_tt_gen, (size_t)grid * warps * sizeof(uint32_t)));
+        TD_CHECK(cudaMallocAsync(&ps.d_tt, words * sizeof(uint64_t), ps.stream));
+        TD_CHECK(cudaMallocAsync(&ps.d_tt_gen, (size_t)grid * warps * sizeof(uint32_t), ps.stream));
         TD_CHECK(cudaMemsetAsync(ps.d_tt, 0, words * sizeof(uint64_t), ps.stream));
         TD_CHECK(cudaMemsetAsync(ps.d_tt_gen, 0, (size_t)grid * warps * sizeof(uint32_t), ps.stream));
         ps.tt_warps = (size_t)grid * warps;
@@ -195,6 +198,7 @@ int percall_start(PercallServer &ps, int device, char *err, size_t errlen) {
     std::memset(&ctl, 0, sizeof ctl);
     ctl.available = ctl.claimed = ps.published;
     ps.h_ctl->stop = 0;
+    ps.h_ctl->exit_reason = 0;
     __atomic_store_n(const_cast<unsigned long long *>(&ps.h_ctl->published), ps.published, __ATOMIC_RELEASE);
     TD_CHECK(cudaMemcpyAsync(ps.d_ctl, &ctl, sizeof ctl, cudaMemcpyHostToDevice, ps.stream));
     TD_CHECK(cudaStreamSynchronize(ps.stream));  // `ctl` lives on this stack
@@ -205,9 +209,11 @@ int percall_start(PercallServer &ps, int device, char *err, size_t errlen) {
     td_serve_kernel<TD_SERVE_PER_REQUEST><<<grid, warps * 32, smem, ps.stream>>>(
         ps.d_ring, ps.d_res, ps.d_done, kPercallRing, ps.d_hctl, ps.d_ctl, ps.d_queue, ps.d_state, ps.d_pool,
         ps.d_items, ps.d_ready, kPercallItems, cfg.serve_grain, cfg.serve_split_level, cfg.serve_check_every, 0,
-        life_ns, cfg.tt_bits > 0 ? ps.d_tt : nullptr, ps.d_tt_gen, cfg.tt_bits, cfg.restart_base, request_ns);
+        life_ns, cfg.tt_bits > 0 ? ps.d_tt : nullptr, ps.d_tt_gen, cfg.tt_bits, cfg.restart_base, request_ns,
+        (uint64_t)g_percall_idle_ns.load());
     TD_CHECK(cudaGetLastError());
     ps.grid = grid;
+    ps.warps = warps;
     ps.running = true;
     ps.retiring = false;
     ps.started = std::chrono::steady_clock::now();
@@ -227,14 +233,68 @@ void percall_park(int device) {
 
 // Stops and frees every per-call launch (td_destroy, td_init_slots).
 void percall_shutdown() {
+    // every launch is stopped before anything is freed: a free waits for all
+    // work on its device
     for (auto &pd : g_percall) {
         std::lock_guard<std::mutex> g(pd.mu);
-        for (auto &ps : pd.srv) {
-            percall_stop(ps);
-            percall_free(ps);
-        }
+        for (auto &ps : pd.srv) percall_stop(ps);
+    }
+    for (auto &pd : g_percall) {
+        std::lock_guard<std::mutex> g(pd.mu);
+        for (auto &ps : pd.srv) percall_free(ps);
         pd.cur = 0;
     }
+}
+
+// Publishes `x` to the device's current launch (starting or replacing it as
+// needed).  Called with the device's lock held.
+int percall_submit(PercallDevice &pd, int device, const td_instance &x, PercallServer **out_ps,
+                   unsigned long long *out_ticket, unsigned *out_gen, char *err, size_t errlen) {
+    TD_CHECK(cudaSetDevice(device));
+    PercallServer *ps = &pd.srv[pd.cur];
+    if (ps->running && cudaStreamQuery(ps->stream) != cudaErrorNotReady) {
+        // the launch has ended (idle, its deadline, or an error): start afresh
+        cudaStreamSynchronize(ps->stream);
+        ps->running = false;
+        ps->retiring = false;
+    }
+    if (ps->running && std::chrono::steady_clock::now() - ps->started > percall_rotate_after()) {
+        PercallServer &next = pd.srv[1 - pd.cur];
+        if (next.running && cudaStreamQuery(next.stream) != cudaErrorNotReady) {
+            cudaStreamSynchronize(next.stream);
+            next.running = false;
+            next.retiring = false;
+        }
+        if (!next.running) {
+            const int rc = percall_start(next, device, err, errlen);
+            if (rc != TD_OK) return rc;
+            if (ps->inflight == 0) percall_stop(*ps);
+            else ps->retiring = true;
+            pd.cur = 1 - pd.cur;
+            ps = &next;
+        }
+    }
+    if (!ps->running) {
+        const int rc = percall_start(*ps, device, err, errlen);
+        if (rc != TD_OK) return rc;
+    }
+    const unsigned long long ticket = ps->published;
+    const unsigned slot = (unsigned)(ticket % kPercallRing);
+    // the ring slot's previous request must have been read (a ring of 2^16
+    // requests makes this wait practically never happen)
+    if (ticket >= kPercallRing)
+        while (__atomic_load_n(&ps->taken[slot], __ATOMIC_ACQUIRE) != ticket - kPercallRing + 1)
+            std::this_thread::yield();
+    ps->h_ring[slot] = x;
+    __atomic_store_n(&ps->h_done[slot], 0ull, __ATOMIC_RELAXED);
+    __atomic_thread_fence(__ATOMIC_SEQ_CST);
+    ps->published = ticket + 1;
+    __atomic_store_n(const_cast<unsigned long long *>(&ps->h_ctl->published), ticket + 1, __ATOMIC_RELEASE);
+    ++ps->inflight;
+    *out_ps = ps;
+    *out_ticket = ticket;
+    *out_gen = ps->generation.load();
+    return TD_OK;
 }
 
 // One blocking search through the device's per-call server.  `x` is the
@@ -245,82 +305,59 @@ int percall_search(int device, const td_instance &x, td_result *out, char *err, 
         return TD_INVALID_ARG;
     }
     PercallDevice &pd = g_percall[device];
-    PercallServer *ps;
-    unsigned long long ticket;
-    unsigned gen;
-    {
-        std::lock_guard<std::mutex> g(pd.mu);
-        TD_CHECK(cudaSetDevice(device));
-        ps = &pd.srv[pd.cur];
-        if (ps->running && cudaStreamQuery(ps->stream) != cudaErrorNotReady) {
-            // the launch has ended (its deadline, or an error): start afresh
-            cudaStreamSynchronize(ps->stream);
-            ps->running = false;
-        }
-        if (ps->running && std::chrono::steady_clock::now() - ps->started > percall_rotate_after()) {
-            PercallServer &next = pd.srv[1 - pd.cur];
-            if (!next.running) {
-                const int rc = percall_start(next, device, err, errlen);
-                if (rc != TD_OK) return rc;
-                if (ps->inflight == 0) percall_stop(*ps);
-                else ps->retiring = true;
-                pd.cur = 1 - pd.cur;
-                ps = &next;
-            }
-        }
-        if (!ps->running) {
-            const int rc = percall_start(*ps, device, err, errlen);
+    // a launch that exits for being idle just as a request is published does
+    // not serve it; the request then goes to a fresh launch (a few tries)
+    for (int attempt = 0;; ++attempt) {
+        PercallServer *ps;
+        unsigned long long ticket;
+        unsigned gen;
+        {
+            std::lock_guard<std::mutex> g(pd.mu);
+            const int rc = percall_submit(pd, device, x, &ps, &ticket, &gen, err, errlen);
             if (rc != TD_OK) return rc;
         }
-        ticket = ps->published;
         const unsigned slot = (unsigned)(ticket % kPercallRing);
-        // the ring slot's previous request must have been read (a ring of 2^16
-        // requests makes this wait practically never happen)
-        if (ticket >= kPercallRing)
-            while (__atomic_load_n(&ps->taken[slot], __ATOMIC_ACQUIRE) != ticket - kPercallRing + 1)
-                std::this_thread::yield();
-        ps->h_ring[slot] = x;
-        __atomic_store_n(&ps->h_done[slot], 0ull, __ATOMIC_RELAXED);
-        __atomic_thread_fence(__ATOMIC_SEQ_CST);
-        ps->published = ticket + 1;
-        __atomic_store_n(const_cast<unsigned long long *>(&ps->h_ctl->published), ticket + 1, __ATOMIC_RELEASE);
-        ++ps->inflight;
-        gen = ps->generation.load();
-    }
-    const unsigned slot = (unsigned)(ticket % kPercallRing);
-    int rc = TD_OK;
-    for (unsigned spin = 1;; ++spin) {
-        if (__atomic_load_n(&ps->h_done[slot], __ATOMIC_ACQUIRE) == ticket + 1) {
-            std::memcpy(out, (const void *)&ps->h_res[slot], sizeof(td_result));
-            break;
-        }
-        if ((spin & 1023u) == 0) {
-            // the launch this request went to has ended (its deadline, an
-            // error) or been replaced after it ended: the request is lost
-            const cudaError_t q = ps->generation.load() != gen ? cudaSuccess : cudaStreamQuery(ps->stream);
-            if (q != cudaErrorNotReady) {
-                if (__atomic_load_n(&ps->h_done[slot], __ATOMIC_ACQUIRE) == ticket + 1) continue;
-                if (q == cudaSuccess) {
-                    set_err(err, errlen, "GPU sorting search deadline reached (the per-call server ended)");
-                    rc = TD_TIMEOUT;
-                } else {
-                    set_err(err, errlen, cuda_msg(q, __FILE__, __LINE__));
-                    rc = TD_CUDA_ERROR;
-                }
+        int rc = TD_OK;
+        bool again = false;
+        for (unsigned spin = 1;; ++spin) {
+            if (__atomic_load_n(&ps->h_done[slot], __ATOMIC_ACQUIRE) == ticket + 1) {
+                std::memcpy(out, (const void *)&ps->h_res[slot], sizeof(td_result));
                 break;
             }
+            if ((spin & 1023u) == 0) {
+                // the launch this request went to has ended, or been replaced
+                // after it ended, without serving it
+                const cudaError_t q = ps->generation.load() != gen ? cudaSuccess : cudaStreamQuery(ps->stream);
+                if (q != cudaErrorNotReady) {
+                    if (__atomic_load_n(&ps->h_done[slot], __ATOMIC_ACQUIRE) == ticket + 1) continue;
+                    // a launch that exits for being idle has served everything
+                    // it copied, so this request was published after its last
+                    // look; after any other end (its deadline) searching again
+                    // is harmless, since a search has no side effects
+                    if (q == cudaSuccess && attempt < 8) {
+                        again = true;
+                    } else if (q == cudaSuccess) {
+                        set_err(err, errlen, "GPU sorting search deadline reached (the per-call server ended)");
+                        rc = TD_TIMEOUT;
+                    } else {
+                        set_err(err, errlen, cuda_msg(q, __FILE__, __LINE__));
+                        rc = TD_CUDA_ERROR;
+                    }
+                    break;
+                }
+            }
+            // spin briefly (a typical search answers within tens of us), then yield
+            if (spin < 4096) __builtin_ia32_pause();
+            else std::this_thread::yield();
         }
-        // spin briefly (a typical search answers within tens of us), then yield
-        if (spin < 4096) __builtin_ia32_pause();
-        else std::this_thread::yield();
+        __atomic_store_n(&ps->taken[slot], ticket + 1, __ATOMIC_RELEASE);
+        {
+            std::lock_guard<std::mutex> g(pd.mu);
+            --ps->inflight;
+            if (ps->retiring && ps->inflight == 0) percall_stop(*ps);
+        }
+        if (!again) return rc;
     }
-    __atomic_store_n(&ps->taken[slot], ticket + 1, __ATOMIC_RELEASE);
-    {
-        std::lock_guard<std::mutex> g(pd.mu);
-        --ps->inflight;
-        if (ps->retiring && ps->inflight == 0) percall_stop(*ps);
-    }
-    return rc;
 }
 
 }  // namespace
@@ -328,12 +365,105 @@ int percall_search(int device, const td_instance &x, td_result *out, char *err, 
 // Per-call searches (td_search, td_search_ordered): mode 1 (default) through
 // the device's resident server, 0 with one launch per call on the slot's
 // stream.  rotate_after_s > 0 sets the age at which a server launch is
-// replaced by a fresh one (default 300 s); 0 keeps the current setting.
-TD_API int td_configure_percall(int mode, double rotate_after_s) {
-    if ((mode != 0 && mode != 1) || rotate_after_s < 0) return TD_INVALID_ARG;
+// replaced by a fresh one (default 300 s); idle_exit_s > 0 the idle time after
+// which a launch with no work left exits by itself (default 0.005 s); 0 keeps
+// the current setting.
+TD_API int td_configure_percall(int mode, double rotate_after_s, double idle_exit_s) {
+    if ((mode != 0 && mode != 1) || rotate_after_s < 0 || idle_exit_s < 0) return TD_INVALID_ARG;
     if (rotate_after_s > 0) g_percall_rotate_ns.store((long long)(rotate_after_s * 1e9));
+    if (idle_exit_s > 0) g_percall_idle_ns.store((long long)(idle_exit_s * 1e9));
     g_percall_mode.store(mode);
     if (mode == 0)
         for (int d = 0; d < kPercallDevices; ++d) percall_park(d);
+    return TD_OK;
+}
+
+// Open-loop Poisson stream through the per-call server, measured from the
+// clients' side: `clients` host threads, client c owning requests c,
+// c + clients, ...; each waits for its request's arrival time, submits it the
+// way td_search does and polls only its own ticket.  Latency runs from the
+// arrival to the client holding the result, so it includes the time a request
+// waited for its client.  Results land in results[i]; stats as for
+// td_serve_open_loop (max_inflight = clients, workers = the server's warps).
+TD_API int td_percall_open_loop(int device, const td_instance *instances, int count, double rate, uint64_t seed,
+                                int clients, td_result *results, td_serve_stats *stats, char *err, size_t errlen) {
+    if (count <= 0 || rate <= 0 || clients <= 0 || !instances || !results || device < 0 ||
+        device >= kPercallDevices) {
+        set_err(err, errlen, "invalid open-loop arguments");
+        return TD_INVALID_ARG;
+    }
+    {
+        std::lock_guard<std::mutex> g(g_mu);
+        const int rc = ensure_device(device, err, errlen);
+        if (rc != TD_OK) return rc;
+    }
+    // start the server before the clock runs
+    td_result warm;
+    td_instance probe = instances[0];
+    int rc = percall_search(device, probe, &warm, err, errlen);
+    if (rc != TD_OK) return rc;
+    std::vector<double> arrive(count), submitted(count), completed(count);
+    uint64_t st = seed;
+    double t = 0;
+    for (int i = 0; i < count; ++i) {
+        const double u = ((splitmix64(st) >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+        t += -std::log(u) / rate;
+        arrive[i] = t;
+    }
+    std::atomic<int> failed{0};
+    std::string first_err;
+    std::mutex err_mu;
+    const auto t0 = std::chrono::steady_clock::now();
+    auto now_s = [&] { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
+    auto client = [&](int c) {
+        char cerr[256];
+        for (int i = c; i < count && !failed.load(); i += clients) {
+            while (now_s() < arrive[i]) {
+            }
+            submitted[i] = now_s();
+            const int r = percall_search(device, instances[i], &results[i], cerr, sizeof cerr);
+            completed[i] = now_s();
+            if (r != TD_OK) {
+                std::lock_guard<std::mutex> g(err_mu);
+                if (!failed.exchange(1)) first_err = cerr;
+            }
+        }
+    };
+    std::vector<std::thread> th;
+    for (int c = 0; c < clients; ++c) th.emplace_back(client, c);
+    for (auto &x : th) x.join();
+    const double wall = now_s();
+    if (failed.load()) {
+        set_err(err, errlen, first_err);
+        return TD_TIMEOUT;
+    }
+    std::vector<double> lat(count);
+    double wait = 0, sum = 0;
+    uint64_t found = 0;
+    for (int i = 0; i < count; ++i) {
+        lat[i] = (completed[i] - arrive[i]) * 1e3;
+        wait += (submitted[i] - arrive[i]) * 1e3;
+        sum += lat[i];
+        found += results[i].status == TD_FOUND;
+    }
+    std::sort(lat.begin(), lat.end());
+    auto pct = [&](double q) { return lat[std::min<size_t>(lat.size() - 1, (size_t)(q * (lat.size() - 1) + 0.5))]; };
+    if (stats) {
+        stats->p50_ms = pct(0.50);
+        stats->p99_ms = pct(0.99);
+        stats->p999_ms = pct(0.999);
+        stats->mean_ms = sum / count;
+        stats->max_ms = lat.back();
+        stats->offered_per_s = count / arrive[count - 1];
+        stats->served_per_s = count / wall;
+        stats->wall_s = wall;
+        stats->admission_wait_ms_mean = wait / count;
+        stats->served = (uint64_t)count;
+        stats->found = found;
+        stats->max_inflight = clients;
+        std::lock_guard<std::mutex> g(g_percall[device].mu);
+        const PercallServer &ps = g_percall[device].srv[g_percall[device].cur];
+        stats->workers = ps.grid * ps.warps - 1;
+    }
     return TD_OK;
 }

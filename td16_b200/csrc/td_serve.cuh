@@ -15,8 +15,13 @@
 struct td_serve_host_ctl {     // pinned, mapped: written by the host
     volatile unsigned long long published;
     volatile int stop;
-    int pad;
+    volatile int exit_reason;  // written by the dispatcher as it exits (TD_SERVE_EXIT_*)
 };
+
+// Why a serving launch's dispatcher stopped.
+#define TD_SERVE_EXIT_IDLE 1      // no request for the idle time and no work left
+#define TD_SERVE_EXIT_STOP 2      // the host asked
+#define TD_SERVE_EXIT_DEADLINE 3  // the launch deadline passed
 
 struct td_serve_dev_ctl {      // device memory: scheduler state of the launch
     unsigned long long available;
@@ -71,7 +76,7 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
                                                       int grain, int max_level, int check_every, uint64_t max_exp,
                                                       uint64_t time_limit_ns, uint64_t *tt, uint32_t *tt_gen,
                                                       int tt_bits, uint32_t restart_base,
-                                                      uint64_t request_limit_ns) {
+                                                      uint64_t request_limit_ns, uint64_t idle_exit_ns) {
     constexpr bool ALL_ORDERED = MODE == TD_SERVE_ORDERED;
     extern __shared__ __align__(16) uint8_t td_smem[];
     const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -84,6 +89,7 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
         // ticket (0, or where the previous launch of a per-call server ended)
         unsigned long long avail = *(volatile unsigned long long *)&dctl->available;
         unsigned backoff = 256;
+        uint64_t last_request = td_globaltimer();
         for (;;) {
             const int hstop = hctl->stop;
             const unsigned long long pub = hctl->published;  // read after stop: a stop is never ahead of its requests
@@ -97,15 +103,34 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
                 if (lane == 0) atomicExch(&dctl->available, pub);
                 avail = pub;
                 backoff = 256;
+                last_request = td_globaltimer();
                 continue;
             }
+            int reason = 0;
+            const uint64_t now = td_globaltimer();
             if (hstop) {
-                if (lane == 0) atomicExch(&dctl->stop, 1);
-                break;
+                reason = TD_SERVE_EXIT_STOP;
+            } else if (now > deadline) {
+                reason = TD_SERVE_EXIT_DEADLINE;
+            } else if (idle_exit_ns && now - last_request > idle_exit_ns) {
+                // idle: leave once every request copied so far is finished, so
+                // that a device-wide synchronisation elsewhere in the process
+                // waits for this launch no longer than the idle time.  A
+                // request published after the last read above is not served;
+                // its client sees the launch end without its result and
+                // submits it again to a fresh launch.
+                int quiet = 0;
+                if (lane == 0)
+                    quiet = *(volatile unsigned long long *)&dctl->claimed >= avail &&
+                            *(volatile int *)&pool->active == 0 &&
+                            *(volatile int *)&pool->consumed >= *(volatile int *)&pool->produced;
+                if (__shfl_sync(TD_FULL, quiet, 0)) reason = TD_SERVE_EXIT_IDLE;
             }
-            if (td_globaltimer() > deadline) {
+            if (reason) {
                 if (lane == 0) {
-                    td_serve_record(dctl, pool, 1, -1);
+                    if (reason == TD_SERVE_EXIT_DEADLINE) td_serve_record(dctl, pool, 1, -1);
+                    hctl->exit_reason = reason;
+                    __threadfence_system();
                     atomicExch(&dctl->stop, 1);
                 }
                 break;
@@ -440,12 +465,12 @@ TD_API int td_serve_open(int device, unsigned ring_size, unsigned flags, double 
         td_serve_kernel<TD_SERVE_ORDERED><<<grid, warps * 32, smem, sv->stream>>>(
             sv->d_ring, sv->d_res, sv->d_done, ring_size, sv->d_hctl, sv->d_ctl, sv->d_queue, sv->d_state,
             sv->d_pool, sv->d_items, sv->d_ready, sv->item_capacity, cfg.serve_grain, cfg.serve_split_level,
-            cfg.serve_check_every, 0, limit_ns, nullptr, nullptr, 0, 0u, 0ull);
+            cfg.serve_check_every, 0, limit_ns, nullptr, nullptr, 0, 0u, 0ull, 0ull);
     else
         td_serve_kernel<TD_SERVE_FREE><<<grid, warps * 32, smem, sv->stream>>>(
             sv->d_ring, sv->d_res, sv->d_done, ring_size, sv->d_hctl, sv->d_ctl, sv->d_queue, sv->d_state,
             sv->d_pool, sv->d_items, sv->d_ready, sv->item_capacity, cfg.serve_grain, cfg.serve_split_level,
-            cfg.serve_check_every, 0, limit_ns, sv->d_tt, sv->d_tt_gen, tt_bits, 0u, 0ull);
+            cfg.serve_check_every, 0, limit_ns, sv->d_tt, sv->d_tt_gen, tt_bits, 0u, 0ull, 0ull);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, __LINE__);
     *handle = sv;
     return TD_OK;

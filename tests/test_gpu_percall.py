@@ -158,3 +158,27 @@ def test_per_call_edge_cases_through_the_server(slots):
         td.search(0, bytes([0, 1, 2]), bytes([1, 2, 0]), 1, 2.0, 10)
     with pytest.raises(td.TdError):
         td.search(SLOTS, bytes([0, 1, 2]), bytes([1, 2, 0]), 1, 2.0, 1)
+
+
+def test_idle_server_exits_and_restarts(slots):
+    """The per-call launch exits by itself once idle (5 ms here by default),
+    so a device-wide synchronisation afterwards returns at once; searches
+    spaced further apart than that each start it again and stay correct."""
+    import time
+    import torch
+    td = slots
+    perms, n = td.synth_perms(2, 256, 16, 16, 50, 1, 4)
+    beta = np.zeros((256, 17), np.uint8)
+    omega = np.zeros((256, 17), np.uint8)
+    init = (td.prepare_perms(perms, n, 9)["packed"] & 31).astype(np.int32)
+    td._lib.lib().td_pairs_from_perms(256, perms.ctypes.data, n.ctypes.data, beta.ctypes.data, omega.ctypes.data)
+    r = _run(td, "td_search", beta, omega, 17, init, 9)
+    assert (r["status"] == 1).all()
+    time.sleep(0.05)
+    t0 = time.perf_counter()
+    torch.cuda.synchronize()
+    assert time.perf_counter() - t0 < 0.5
+    for i in range(24):  # each of these finds the launch gone and starts a new one
+        time.sleep(0.01)
+        moves = td.search(i % SLOTS, beta[i].tobytes(), omega[i].tobytes(), int(init[i]), 0.0, 9)
+        assert 1 <= len(moves) <= 9

@@ -108,13 +108,16 @@ def test_accept_blocks_while_batches_wait(td):
 
 @pytest.mark.gpu
 def test_batched_consumer_matches_per_call_search(td, oracle):
-    """2,048 pairs of the n = 11..13 mix from 8 generator threads: the same
-    verdicts as per-call td_search and the oracle; every witness replays."""
-    perms, n = td.synth_perms(1, 2048, 11, 13, 25, 1, 3)
+    """2,048 pairs from 8 generator threads, half of the n = 11..13 mix at
+    bound floor(n/2)+1 and half hard n = 13 pairs at bound 6 (most without a
+    witness): the same verdicts as per-call td_search and the oracle; every
+    witness replays."""
+    p1, n1 = td.synth_perms(1, 1024, 11, 13, 25, 1, 3)
+    p2, n2 = td.synth_perms(5, 1024, 13, 13, 100, 1, 3)
     pairs = []
-    for p, k in zip(perms, n):
+    for (p, k), bound in [((p, k), int(k // 2 + 1)) for p, k in zip(p1, n1)] + [((p, k), 6) for p, k in zip(p2, n2)]:
         beta, omega, init = oracle.perm_to_pair(p[:k].tolist())
-        pairs.append((bytes(beta), bytes(omega), init, int(k // 2 + 1)))
+        pairs.append((bytes(beta), bytes(omega), init, bound))
     td.init_slots(4, [0], 256 << 20)
     sunk = []
     try:
