@@ -168,6 +168,14 @@ TD_API int td_replay_symbols_device(int count, const uint8_t *d_beta, const uint
     return 0;
 }
 
+// Loads the replay kernel on the current device (called when the engine sets
+// a device up, so that its first launch never waits for loading while the
+// per-call server's resident launch runs).  Returns a cudaError_t.
+int td_cert_preload(void) {
+    cudaFuncAttributes a;
+    return (int)cudaFuncGetAttributes(&a, td_replay_symbols_kernel);
+}
+
 // ---- batched certificate sink ----------------------------------------------
 //
 // AsyncCertificateWriter semantics (AsyncCertificateWriter.java:50-116): one

@@ -564,6 +564,12 @@ uint64_t time_limit_ns() {
     return v;
 }
 
+// Loads every kernel of the library on the current device (defined at the
+// end of this file).  With lazy module loading a kernel's code would
+// otherwise be loaded at its first launch, which may wait for the work
+// already on the device, the per-call server's resident launch included.
+int preload_kernels(char *err, size_t errlen);
+
 // The launch settings of one launch, read together under g_mu so that a
 // concurrent td_configure_* call never hands a launch half of its change.
 struct LaunchCfg {
@@ -631,6 +637,8 @@ int ensure_device(int device, char *err, size_t errlen) {
     TD_CHECK(cudaFuncSetAttribute(td_persistent_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
     TD_CHECK(cudaFuncSetAttribute(td_persistent_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
     TD_CHECK(cudaFuncSetAttribute(td_steal_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
+    const int rc = preload_kernels(err, errlen);
+    if (rc != TD_OK) return rc;
     d.ready = true;
     return TD_OK;
 }
@@ -1659,3 +1667,30 @@ TD_API int td_batch_graph_destroy(void *graph) {
 
 #include "td_serve.cuh"
 #include "td_percall.cuh"
+
+// defined in td_cert.cu
+int td_cert_preload(void);
+
+namespace {
+
+int preload_kernels(char *err, size_t errlen) {
+    cudaFuncAttributes a;
+    TD_CHECK(cudaFuncGetAttributes(&a, td_plain_kernel<true>));
+    TD_CHECK(cudaFuncGetAttributes(&a, td_plain_kernel<false>));
+    TD_CHECK(cudaFuncGetAttributes(&a, td_persistent_kernel<true>));
+    TD_CHECK(cudaFuncGetAttributes(&a, td_persistent_kernel<false>));
+    TD_CHECK(cudaFuncGetAttributes(&a, td_steal_kernel));
+    TD_CHECK(cudaFuncGetAttributes(&a, td_epoch_kernel));
+    TD_CHECK(cudaFuncGetAttributes(&a, td_finalize_kernel));
+    TD_CHECK(cudaFuncGetAttributes(&a, td_count_kernel));
+    TD_CHECK(cudaFuncGetAttributes(&a, td_validate_kernel));
+    TD_CHECK(cudaFuncGetAttributes(&a, td_int_peak_kernel<0>));
+    TD_CHECK(cudaFuncGetAttributes(&a, td_int_peak_kernel<1>));
+    TD_CHECK(cudaFuncGetAttributes(&a, td_serve_kernel<TD_SERVE_FREE>));
+    TD_CHECK(cudaFuncGetAttributes(&a, td_serve_kernel<TD_SERVE_ORDERED>));
+    TD_CHECK(cudaFuncGetAttributes(&a, td_serve_kernel<TD_SERVE_PER_REQUEST>));
+    TD_CHECK((cudaError_t)td_cert_preload());
+    return TD_OK;
+}
+
+}  // namespace
