@@ -473,3 +473,7 @@ extern "C" int td_emu_search_batch(int count, const td_instance *x, unsigned fla
     for (auto &t : pool) t.join();
     return 0;
 }
+
+// The engine's device replay of a witness (td_witness_ok, the rule of
+// TD_FLAG_VERIFY), for the CPU tests.
+extern "C" int td_emu_witness_ok(const td_instance *x, const td_result *r) { return td_witness_ok(*x, *r); }

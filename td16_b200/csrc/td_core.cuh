@@ -336,6 +336,38 @@ TD_HD int td_accepts(int N, int init, float min_rate, int full, int odd, int dep
     return gained > 0 && ratio >= min_rate;
 }
 
+// Odd-length cycles of omega for the pinned state (L, off) over N symbols,
+// and a bit per caller position whose symbol omega fixes.  Beta reads B = (0,
+// L[0]+1, ..., L[N-2]+1) from pinned position 0, caller position c sits at
+// pinned position (c + off) mod N, and omega(B[p]) = B[p-1] + 1 (mod N).
+TD_HD int td_pinned_cycles(uint64_t L, int off, int N, uint32_t *fixed_at_caller) {
+    uint8_t B[TD_MAX_N], om[TD_MAX_N];
+    for (int p = 0; p < N; ++p) B[p] = p ? (uint8_t)(td_nib(L, p - 1) + 1) : 0;
+    uint32_t fixed = 0;
+    for (int p = 0; p < N; ++p) {
+        const int prev = B[p == 0 ? N - 1 : p - 1] + 1;
+        om[B[p]] = (uint8_t)(prev == N ? 0 : prev);
+        if (om[B[p]] == B[p]) {
+            int c = p - off;
+            c += c < 0 ? N : 0;
+            fixed |= 1u << c;
+        }
+    }
+    uint32_t seen = 0;
+    int odd = 0;
+    for (int x = 0; x < N; ++x) {
+        if ((seen >> x) & 1u) continue;
+        int len = 0;
+        for (int y = x; !((seen >> y) & 1u); y = om[y]) {
+            seen |= 1u << y;
+            ++len;
+        }
+        odd += len & 1;
+    }
+    *fixed_at_caller = fixed;
+    return odd;
+}
+
 TD_HD int td_can_reach(int N, int init, float min_rate, int max_depth, int full,
                        int odd, int depth) {
     const int missing = N - odd;
@@ -350,6 +382,36 @@ TD_HD int td_can_reach(int N, int init, float min_rate, int max_depth, int full,
         if (best < min_rate) return 0;
     }
     return 1;
+}
+
+// Replay of a witness with the search's own rules: every move is an in-range
+// position triple i<j<k whose symbols omega does not fix and whose odd-cycle
+// change is 0 or +2 (sorting_search.cu:375-380,608-610), there are at most
+// max_moves of them, and the last node passes the instance's acceptance test
+// (satisfies_rate, sorting_search.cu:336-346; with full sorting, omega = id).
+// With full sorting this is CertificateValidator's replay
+// (CertificateValidator.java:14-50) in pinned form.
+TD_HD int td_witness_ok(const td_instance &x, const td_result &r) {
+    const int N = x.n_symbols;
+    if (!(r.status == TD_FOUND && r.depth >= 1 && r.depth <= x.max_moves && N >= 3 && N <= TD_MAX_N)) return 0;
+    uint64_t L = x.perm;
+    int off = x.offset;
+    uint32_t fixed = 0;
+    int odd = td_pinned_cycles(L, off, N, &fixed);
+    for (int d = 0; d < r.depth; ++d) {
+        const int m = r.moves[d];
+        const int i = m & 31, j = (m >> 5) & 31, k = (m >> 10) & 31;
+        if (!(i < j && j < k && k < N) || (((fixed >> i) | (fixed >> j) | (fixed >> k)) & 1u)) return 0;
+        uint64_t nL;
+        int noff;
+        td_apply_move(L, off, N, i, j, k, &nL, &noff);
+        L = nL;
+        off = noff;
+        const int nodd = td_pinned_cycles(L, off, N, &fixed);
+        if (nodd != odd && nodd != odd + 2) return 0;
+        odd = nodd;
+    }
+    return td_accepts(N, td_inst_init(x), x.min_rate, td_inst_full(x), odd, r.depth);
 }
 
 // ---- instance preparation (host side) --------------------------------------

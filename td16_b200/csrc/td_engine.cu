@@ -401,32 +401,20 @@ __global__ void __launch_bounds__(256) td_count_kernel(const td_result *__restri
     }
 }
 
-// Witness replay in pinned form: every move must be an in-range position
-// triple i<j<k, at most max_moves of them, and the final state must be the
-// identity (omega = id  <=>  beta = rho  <=>  L = 0,1,...,n-1).
+// Witness replay in pinned form with the search's own rules: every move is an
+// in-range position triple i<j<k whose symbols omega does not fix and whose
+// odd-cycle change is 0 or +2 (sorting_search.cu:375-380,608-610), there are
+// at most max_moves of them, and the last node passes the acceptance test of
+// the instance (satisfies_rate, sorting_search.cu:336-346: with full sorting,
+// omega = id).  With full sorting this is CertificateValidator's replay
+// (CertificateValidator.java:14-50) in pinned form.
 __global__ void td_validate_kernel(const td_instance *__restrict__ in, td_result *__restrict__ res,
                                    uint8_t *__restrict__ ok, int count, int mark) {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= count) return;
     const td_instance x = in[idx];
     const td_result r = res[idx];
-    const int N = x.n_symbols;
-    uint8_t good = r.status == TD_FOUND && r.depth >= 1 && r.depth <= x.max_moves && N >= 3 && N <= TD_MAX_N;
-    uint64_t L = x.perm;
-    int off = x.offset;
-    for (int d = 0; good && d < r.depth; ++d) {
-        const int m = r.moves[d];
-        const int i = m & 31, j = (m >> 5) & 31, k = (m >> 10) & 31;
-        if (!(i < j && j < k && k < N)) { good = 0; break; }
-        uint64_t nL;
-        int noff;
-        td_apply_move(L, off, N, i, j, k, &nL, &noff);
-        L = nL;
-        off = noff;
-    }
-    uint64_t ident = 0;
-    for (int m = 0; m < 16; ++m) ident |= (uint64_t)m << (4 * m);
-    good = good && L == ident;
+    const uint8_t good = (uint8_t)td_witness_ok(x, r);
     if (ok) ok[idx] = good;
     if (mark && r.status == TD_FOUND && !good) res[idx].status = TD_ERR_VERIFY;
 }

@@ -188,3 +188,43 @@ def test_per_call_path_reproduces_reference_kernel(td, oracle):
                     assert _witness_ok(oracle, c, moves), (name, c)
     finally:
         td.destroy()
+
+
+def test_device_replay_rule_accepts_every_reference_witness_and_rejects_tampering(emu):
+    """td_witness_ok, the rule behind TD_FLAG_VERIFY and td_validate_batch_device
+    (run here on the host through the emulator): every witness the reference
+    kernel returned passes, in full and partial sorting; a witness with a move
+    dropped, a move out of range, a depth beyond the bound or a rate it misses
+    does not."""
+    from tests.test_engine_logic_cpu import Inst, Res, _u8
+    checked = rejected = 0
+    for name in ORDERED_SETS + VERDICT_SETS:
+        for c in FIX[name]:
+            if not c["moves"]:
+                continue
+            x = Inst()
+            assert emu.td_emu_prepare_pair(_u8(c["beta"]), _u8(c["omega"]), len(c["beta"]), c["init"],
+                                           C.c_float(c["rate"]), c["maxd"], c["full"], C.byref(x)) == 0
+
+            def rec(moves):
+                r = Res()
+                r.status, r.depth = 1, len(moves)
+                for d, (i, j, k) in enumerate(moves):
+                    r.moves[d] = (i & 31) | ((j & 31) << 5) | ((k & 31) << 10)
+                return r
+
+            moves = [tuple(m) for m in c["moves"]]
+            assert emu.td_emu_witness_ok(C.byref(x), C.byref(rec(moves))) == 1, (name, c)
+            checked += 1
+            bad = [rec(moves[:-1]) if len(moves) > 1 else None,
+                   rec(moves[:-1] + [(0, 1, len(c["beta"]))])]
+            if len(moves) < 9:
+                bad.append(rec(moves + [moves[-1]]))
+            for r in bad:
+                if r is not None:
+                    rejected += emu.td_emu_witness_ok(C.byref(x), C.byref(r)) == 0
+            if c["full"] == 0 and c["rate"] > 0:
+                x2 = Inst.from_buffer_copy(x)
+                x2.min_rate = 100.0  # beyond any gain per move
+                assert emu.td_emu_witness_ok(C.byref(x2), C.byref(rec(moves))) == 0
+    assert checked > 2000 and rejected > 2 * checked * 0.9
