@@ -1,7 +1,9 @@
 """Small, seeded workloads that exercise one kernel each, for profiling with
 ncu (one kernel per command, `-k regex:<kernel>`) and for quick timings.
 
-    python -m td16_b200.profile_cases <case> [--count N]
+    python -m td16_b200.profile_cases <case> [--count N] [--table-bits B]
+
+Every case runs with the benchmark's launch shape (td16_b200/tuned.json).
 
   steal    td_steal_kernel: the S_16 benchmark instances (seed 2, half
            near-reverse), bound 9, free order (default 2^18 instances)
@@ -55,8 +57,12 @@ def _device_batch(inst, flags, slot=0):
     return a.elapsed_time(b), res, d_in, d_out
 
 
-def run(case: str, count: int | None) -> dict:
+def run(case: str, count: int | None, table_bits: int | None = None) -> dict:
     _lib.init_slots(1, [0], 256 << 20)
+    from .autotune import apply
+    tuned = apply("17")  # the benchmark's launch shape (td16_b200/tuned.json)
+    if table_bits is not None:
+        _lib.configure_table(table_bits)
     try:
         if case in ("steal", "plain", "validate"):
             k = count or {"steal": 1 << 18, "plain": 8192, "validate": 1 << 20}[case]
@@ -64,7 +70,8 @@ def run(case: str, count: int | None) -> dict:
             inst = _lib.prepare_perms(perms, n, 9)
             ms, res, d_in, d_out = _device_batch(inst, _lib.FLAG_PLAIN if case == "plain" else 0)
             out = {"case": case, "instances": k, "ms": ms, "found": int((res["status"] == 1).sum()),
-                   "expansions": int(res["expansions"].astype(np.int64).sum())}
+                   "expansions": int(res["expansions"].astype(np.int64).sum()), "launch_shape": tuned,
+                   "table_bits": 12 if table_bits is None else table_bits}
             if case == "validate":
                 import torch
                 ok = torch.zeros(k, dtype=torch.uint8, device="cuda")
@@ -118,9 +125,11 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["steal", "ordered", "plain", "replay", "validate", "serve", "percall"])
     ap.add_argument("--count", type=int, default=None)
+    ap.add_argument("--table-bits", type=int, default=None,
+                    help="entries of the explored-state tables (2^bits per warp; 0 = none; default 12)")
     a = ap.parse_args()
     t0 = time.perf_counter()
-    out = run(a.case, a.count)
+    out = run(a.case, a.count, a.table_bits)
     out["wall_s"] = time.perf_counter() - t0
     print(json.dumps(out), flush=True)
 

@@ -95,19 +95,28 @@ def test_noalloc_calls_leave_device_memory_unchanged(td):
     calls (nothing else allocates inside that window)."""
     import torch
     f = _noalloc(td)
-    perms, n = td.synth_perms(44, 8192, 13, 16, 50, 1, 3)
-    batch = td.prepare_perms(perms, n, (n // 2 + 1).astype(np.int32))
-    d_in = torch.from_numpy(batch.view(np.uint8).copy()).cuda()
-    d_out = torch.zeros(len(batch) * 32, dtype=torch.uint8, device="cuda")
+    # the free order on a mix of hard instances, and the reference order (one
+    # warp per instance, blind) where every search ends quickly
+    p1, n1 = td.synth_perms(44, 8192, 13, 16, 50, 1, 3)
+    free = td.prepare_perms(p1, n1, (n1 // 2 + 1).astype(np.int32))
+    p2, n2 = td.synth_perms(45, 4096, 10, 10, 0, 0, 0)
+    ordered = td.prepare_perms(p2, n2, 6)
+    cases = []
+    for batch, flags in ((free, td._lib.FLAG_VERIFY), (ordered, td._lib.FLAG_ORDERED | td._lib.FLAG_PLAIN)):
+        d_in = torch.from_numpy(batch.view(np.uint8).copy()).cuda()
+        d_out = torch.zeros(len(batch) * 32, dtype=torch.uint8, device="cuda")
+        cases.append((len(batch), d_in, d_out, flags))
     stream = torch.cuda.current_stream().cuda_stream
-    for flags in (td._lib.FLAG_VERIFY, td._lib.FLAG_ORDERED | td._lib.FLAG_PLAIN):
-        rc, msg = _call(f, len(batch), d_in, d_out, flags, stream)   # set-up: first use of each kernel
+    for count, d_in, d_out, flags in cases:  # set-up: first use of each kernel
+        rc, msg = _call(f, count, d_in, d_out, flags, stream)
         assert rc == 0, msg
     torch.cuda.synchronize()
     free_before, _ = torch.cuda.mem_get_info()
-    for flags in (td._lib.FLAG_VERIFY, td._lib.FLAG_ORDERED | td._lib.FLAG_PLAIN):
-        rc, msg = _call(f, len(batch), d_in, d_out, flags, stream)
+    for count, d_in, d_out, flags in cases:
+        rc, msg = _call(f, count, d_in, d_out, flags, stream)
         assert rc == 0, msg
     torch.cuda.synchronize()
     free_after, _ = torch.cuda.mem_get_info()
     assert free_after == free_before
+    for count, _, d_out, _ in cases:
+        assert (_results(d_out)["status"] >= 0).all()
