@@ -39,16 +39,19 @@ METRIC = "verified witnesses/s (S_16, d<=9)"
 UNIT = "witnesses/s"
 WORKLOAD = "full-size decision search: 2^20 S_16 perms, 50% uniform / 50% reverse o 1-4 transpositions, d<=9"
 # Per node expansion at N = 17, the search kernel's warp instructions (all
-# pipes) and those of the integer ALU pipe, and its DRAM bytes per launch:
-# ncu capture of td_steal_kernel on the first 2^18 instances of this workload
-# (tuned launch shape, restarts and explored-state tables on), summarised in
-# profiles/td_steal_kernel_s16_mix_2p18.md: 10.892 G warp instructions over
-# 14.18 M expansions (skipped children, restarts, donation and scheduling
-# included); the ALU pipe busy 55.413% of 2 warp instructions per cycle over
-# 5.262 G SM cycles; 2.01 GB of DRAM traffic, mostly the explored-state tables.
-INST_PER_EXPANSION = 10.892e9 / 14.18e6
-ALU_INST_PER_EXPANSION = 0.55413 * 2 * 5.262e9 / 14.18e6
-DRAM_BYTES_PER_2P18_LAUNCH = 2.01e9
+# pipes) and those of the integer ALU pipe, and its DRAM bytes per launch: one-
+# pass ncu captures of td_steal_kernel on one launch of this benchmark's 2^20-
+# instance batch with the tuned launch shape, summarised with their commands in
+# profiles/td_steal_kernel_s16_2p20_counters.md.  37.697 G warp instructions
+# and 20.491 G ALU-pipe instructions over the launch's 50.03 M expansions
+# (restarts, skipped children, donation and scheduling included) in
+# 95.96 M SM cycles: the ALU pipe busy 72.1 % of its 2 warp instructions per
+# cycle per SM, issue 66.4 % of 4; 0.901 GB read and 0.834 GB written.
+INST_PER_EXPANSION = 37.697e9 / 50.03e6
+ALU_INST_PER_EXPANSION = 20.491e9 / 50.03e6
+ALU_BUSY_MEASURED = 20.491e9 / (95.96e6 * 148 * 2)
+ISSUE_MEASURED = 37.697e9 / (95.96e6 * 148 * 4)
+DRAM_BYTES_PER_LAUNCH = 0.901e9 + 0.834e9
 
 def rank_info():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
@@ -492,9 +495,11 @@ def run_engine(args):
                 "issue_frac": nodes_per_s * INST_PER_EXPANSION / (4 * sms * sm_mhz * 1e6),
                 "issue_lop3_imad_measured": issue_peak.value / 1e9,
                 "inst_per_expansion": INST_PER_EXPANSION,
-                "traffic": DRAM_BYTES_PER_2P18_LAUNCH * count / (1 << 18),
-                "traffic_note": "DRAM bytes per launch: ncu on the first 2^18 instances, scaled by instance count "
-                                "(mostly the explored-state tables)",
+                "traffic": DRAM_BYTES_PER_LAUNCH * count / COUNT,
+                "traffic_note": "DRAM bytes of one 2^20 launch (ncu, one pass, the benchmark launch itself); the "
+                                "algorithmic bytes are 48 per instance (16 in, 32 out): 50 MB; the rest is the "
+                                "explored-state tables (4736 warps x 32 KiB = 155 MB > the 126 MB L2)",
+                "alu_busy_measured": ALU_BUSY_MEASURED, "issue_measured": ISSUE_MEASURED,
                 "nodes_per_s": nodes_per_s, "triples_per_s": triples_per_s}
 
     graph.close()
