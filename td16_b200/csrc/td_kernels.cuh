@@ -586,15 +586,6 @@ struct td_donate_ctx {
     td_inst_state *state;
 };
 
-// Idle checks once idle warps were seen: the interval is divided by
-// TD_TAIL_CHECK_DIV and a donation may give TD_TAIL_GRAIN_MUL times the grain.
-#ifndef TD_TAIL_CHECK_DIV
-#define TD_TAIL_CHECK_DIV 1
-#endif
-#ifndef TD_TAIL_GRAIN_MUL
-#define TD_TAIL_GRAIN_MUL 1
-#endif
-
 #define TD_DFS_FOUND 1
 #define TD_DFS_EXHAUSTED 0
 #define TD_DFS_BUDGET (-2)
@@ -844,11 +835,6 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
     }
     r.expansions = 1;
     int since_check = 0;
-    // expansions until the next idle check: the tuned interval while no warp
-    // waits, shorter once idle warps were seen (the end of a batch, when a
-    // few long searches remain and idle warps wait for their subtrees)
-    int check_next = dc ? dc->check_every : 0;
-    int tail_grain = dc ? dc->grain : 0;
     bool tt_on = false;  // the table is in use (free order, after TD_TT_AFTER expansions)
     uint32_t tt_gen = 0;  // its current generation
     int attempt = 0;     // free order: restarts with another child order (td_attempt_budget)
@@ -883,7 +869,7 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
             }
         }
         if constexpr (!ORDERED) {
-            if (dc && ++since_check >= check_next) {
+            if (dc && ++since_check >= dc->check_every) {
                 since_check = 0;
                 int hungry = 0, stop = 0;
                 if (lane == 0) {
@@ -903,10 +889,8 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
                 // a search that has handed out subtrees no longer restarts: the
                 // subtrees of an abandoned attempt would go on being searched,
                 // and searching in parallel already varies the order
-                if (hungry > 0 && td_donate(s, *dc, code, d0, level, N, min(hungry, tail_grain)) > 0)
+                if (hungry > 0 && td_donate(s, *dc, code, d0, level, N, min(hungry, dc->grain)) > 0)
                     attempt_budget = ~0u;
-                check_next = hungry > 0 ? max(1, dc->check_every / TD_TAIL_CHECK_DIV) : dc->check_every;
-                tail_grain = hungry > 0 ? dc->grain * TD_TAIL_GRAIN_MUL : dc->grain;
             }
         }
         if ((r.expansions & 255u) == 0) {
