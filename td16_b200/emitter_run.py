@@ -143,16 +143,16 @@ def run_consumer(count: int, slots: int, budget: int, out_path: str, seed: int =
     perms, n = _chunk(seed, 0, count)
     beta, omega = _pairs(perms, n)
     init = (_lib.prepare_perms(perms, n, 9)["packed"] & 31).astype(np.int32)
-    lock = threading.Lock()
-    sink_calls = [0]
-
-    def sink(b, o, witness):
-        writer.enqueue(o, witness)
-        with lock:
-            sink_calls[0] += 1
+    def batch_sink(b, o, nsym, status, depth, moves):
+        # found witnesses of a searched batch go to the certificate writer in one call
+        res = _records(np.where(status == _lib.OK, 1, 0), depth, moves)
+        q = _lib.lib().td_cert_writer_enqueue_batch(writer._h, len(status), _lib._ptr(b), _lib._ptr(o),
+                                                    _lib._ptr(nsym), _lib._ptr(res))
+        if q < 0:
+            raise _lib.TdError(_lib.CUDA_ERROR, "certificate sink rejected a batch")
 
     t0 = time.perf_counter()
-    batcher = PairBatcher(range(slots), batch_size=batch, max_delay_s=0.005, sink=sink)
+    batcher = PairBatcher(range(slots), batch_size=batch, max_delay_s=0.005, batch_sink=batch_sink)
     futures = [None] * count
 
     def generate(g):

@@ -274,6 +274,29 @@ class GPUSortingSearch:
         return _lib.positions_to_symbols(beta, positions)
 
 
+def positions_to_symbols_batch(beta: np.ndarray, depth: np.ndarray, moves: np.ndarray) -> np.ndarray:
+    """Position triples -> symbol triples for a whole batch at once
+    (GPUSortingSearch.java:229-238 per pair): beta uint8[c, 17], depth
+    int[c], moves int16[c, 9, 3]; returns uint8[c, 9, 3] (rows past a pair's
+    depth are zero)."""
+    cur = np.array(beta, dtype=np.int16)
+    c, width = cur.shape
+    out = np.zeros((c, 9, 3), np.uint8)
+    rows = np.arange(c)
+    m = np.arange(width, dtype=np.int16)[None, :]
+    for d in range(int(depth.max()) if c else 0):
+        live = depth > d
+        i, j, k = (moves[:, d, q].astype(np.int16)[:, None] for q in range(3))
+        for q in range(3):
+            out[live, d, q] = cur[rows[live], moves[live, d, q]]
+        # block swap: positions i..k-1 take A[j..k-1] then A[i..j-1]
+        inside = (m >= i) & (m < k)
+        src = np.where(inside, np.where(m < i + (k - j), m + (j - i), m - (k - j)), m)
+        nxt = np.take_along_axis(cur, src.astype(np.int64), axis=1)
+        cur = np.where(live[:, None], nxt, cur)
+    return out
+
+
 class PairBatcher:
     """A case consumer that searches pairs in batches.
 
@@ -288,19 +311,21 @@ class PairBatcher:
     with one td_search_pairs call.  `accept` returns a future of the witness
     as symbol triples (a, b, c) on the pair's beta, [] when there is none; the
     optional `sink(beta, omega, witness)` receives every found witness (e.g. a
-    certificate writer).  At most `max_pending` batches wait for a worker;
+    certificate writer), and the optional `batch_sink(beta, omega, n, status,
+    depth, moves)` each searched batch as arrays (position triples).  At most `max_pending` batches wait for a worker;
     `accept` blocks beyond that, like the reference's bounded queue of
     slots + tdp.gpuQueueCapacity jobs.  `search_fn` replaces the engine call
     (the CPU tests use it)."""
 
     def __init__(self, slots, batch_size: int = 4096, max_delay_s: float = 0.002, max_pending: int | None = None,
-                 sink=None, search_fn=None):
+                 sink=None, search_fn=None, batch_sink=None):
         self.slots = list(slots)
         if not self.slots or batch_size <= 0 or max_delay_s <= 0:
             raise ValueError("a batcher needs slots, a positive batch size and a positive delay")
         self.batch_size = int(batch_size)
         self.max_delay_s = float(max_delay_s)
         self.sink = sink
+        self.batch_sink = batch_sink
         self._search = search_fn or _lib.search_pairs
         self._cv = threading.Condition()
         self._open: list = []          # (beta, omega, init, rate, maxd, full, future) of the filling batch
@@ -380,11 +405,14 @@ class PairBatcher:
         messages = {_lib.OVERFLOW: "GPU sorting search queue overflow",
                     _lib.TIMEOUT: "GPU sorting search deadline reached",
                     _lib.INVALID_ARG: "performGpuSortingSearch: invalid input"}
+        depth = np.where(status == _lib.OK, depth, 0)
+        symbols = positions_to_symbols_batch(beta, depth, moves)
+        if self.batch_sink is not None:
+            self.batch_sink(beta, omega, n, status, depth, moves)
         for i, p in enumerate(batch):
             st = int(status[i])
             if st == _lib.OK:
-                positions = [tuple(int(v) for v in moves[i, d]) for d in range(int(depth[i]))]
-                witness = _lib.positions_to_symbols(p[0], positions)
+                witness = [tuple(int(v) for v in symbols[i, d]) for d in range(int(depth[i]))]
                 if self.sink is not None:
                     self.sink(p[0], p[1], witness)
                 p[6].set_result(witness)

@@ -148,3 +148,26 @@ def test_batched_consumer_matches_per_call_search(td, oracle):
     for p, w in zip(pairs, got):
         if w:
             assert oracle.validate(list(p[0]), list(p[1]), w, p[3]) is None
+
+
+def test_batch_symbol_conversion_matches_the_c_abi(td):
+    """host.positions_to_symbols_batch (the consumer's vectorised conversion)
+    gives td_positions_to_symbols's symbol triples for every pair."""
+    from td16_b200.host import positions_to_symbols_batch
+    rng = np.random.default_rng(1)
+    c = 400
+    beta = np.zeros((c, 17), np.uint8)
+    depth = rng.integers(0, 10, c)
+    moves = np.zeros((c, 9, 3), np.int16)
+    sizes = []
+    for r in range(c):
+        N = int(rng.integers(3, 18))
+        sizes.append(N)
+        beta[r, :N] = rng.permutation(N)
+        for d in range(depth[r]):
+            moves[r, d] = sorted(rng.choice(N, 3, replace=False))
+    out = positions_to_symbols_batch(beta, depth, moves)
+    for r in range(c):
+        want = td._lib.positions_to_symbols(bytes(beta[r, : sizes[r]]),
+                                            [tuple(int(v) for v in moves[r, d]) for d in range(depth[r])])
+        assert [tuple(int(v) for v in out[r, d]) for d in range(depth[r])] == want
