@@ -137,7 +137,16 @@ __global__ void __launch_bounds__(256) td_persistent_kernel(const td_instance *_
 // Ends one unit of a shared search: records a found witness (first finder
 // wins), and the unit that finishes the search last writes the final status
 // and the summed expansions.  Returns 1 in the warp that finished last.
-// System-scope fences: `out` may be host memory mapped into the device.
+// HOST_OUT: `out` is host memory mapped into the device (the serving loop), so
+// the fences are system-scope; the batch engine's results are device memory,
+// where device-scope fences order the same writes at a fraction of the cost.
+template <bool HOST_OUT>
+__device__ __forceinline__ void td_unit_fence() {
+    if (HOST_OUT) __threadfence_system();
+    else __threadfence();
+}
+
+template <bool HOST_OUT>
 __device__ __forceinline__ int td_finish_unit(const td_dfs_out &r, td_inst_state *st, td_result *out,
                                               const uint16_t *path) {
     const int lane = threadIdx.x & 31;
@@ -152,9 +161,9 @@ __device__ __forceinline__ int td_finish_unit(const td_dfs_out &r, td_inst_state
     if (win) td_write_result(out, TD_FOUND, r.depth, r.found_move, path, 0, 0, 7);
     __syncwarp();
     if (lane == 0) {
-        __threadfence_system();
+        td_unit_fence<HOST_OUT>();
         last = atomicSub(&st->pending, 1) == 1;
-        if (last) __threadfence_system();
+        if (last) td_unit_fence<HOST_OUT>();
     }
     last = __shfl_sync(TD_FULL, last, 0);
     if (last) {
@@ -280,7 +289,7 @@ __global__ void __launch_bounds__(256, TD_STEAL_MIN_BLOCKS) td_steal_kernel(cons
                 dc.inst = (uint32_t)unit;
                 dc.state = st;
                 const td_dfs_out r = td_dfs<false>(s, lut, code, x.n_symbols, x.max_moves, 0, lim, &dc);
-                td_finish_unit(r, st, &out[unit], s.path);
+                td_finish_unit<false>(r, st, &out[unit], s.path);
             }
         } else {
             // wait until the donor has written the item (bounded)
@@ -332,7 +341,7 @@ __global__ void __launch_bounds__(256, TD_STEAL_MIN_BLOCKS) td_steal_kernel(cons
                     dc.state = st;
                     r = td_dfs<false>(s, lut, code, x.n_symbols, x.max_moves, d0, ilim, &dc);
                 }
-                td_finish_unit(r, st, &out[idx], s.path);
+                td_finish_unit<false>(r, st, &out[idx], s.path);
             }
         }
         if (lane == 0) atomicSub(&pool->active, 1);

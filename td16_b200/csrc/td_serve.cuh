@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
                 if (lane == 0) stop = *(volatile int *)&state[slot].found;
                 run = !__shfl_sync(TD_FULL, stop, 0);
                 if (!run) {  // the request already has its witness
-                    if (td_finish_unit(r, &state[slot], &results[slot], s.path) && lane == 0) {
+                    if (td_finish_unit<true>(r, &state[slot], &results[slot], s.path) && lane == 0) {
                         done[slot] = (unsigned long long)req + 1ull;
                         atomicAdd(&dctl->served, 1ull);
                     }
@@ -313,7 +313,7 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
             ulim.restart_base = kind == 1 ? restart_base : 0;
             if (ord) r = td_dfs<true>(s, lut, code, x.n_symbols, x.max_moves, d0, ulim, nullptr);
             else r = td_dfs<false>(s, lut, code, x.n_symbols, x.max_moves, d0, ulim, &dc);
-            if (td_finish_unit(r, &state[slot], &results[slot], s.path) && lane == 0) {
+            if (td_finish_unit<true>(r, &state[slot], &results[slot], s.path) && lane == 0) {
                 done[slot] = (unsigned long long)req + 1ull;
                 atomicAdd(&dctl->served, 1ull);
             }

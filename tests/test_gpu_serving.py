@@ -107,3 +107,22 @@ def test_ring_slot_is_reused_only_after_its_result_is_taken(td):
     finally:
         td.destroy()
     assert [int(r["status"]) for r in results] == [int(s) for s in batch["status"]]
+
+
+def test_client_side_open_loop_through_the_per_call_server(td, oracle):
+    """An open-loop Poisson stream through the per-call server, 8 client
+    threads each polling only its own requests (td_percall_open_loop): every
+    request is served, verdicts equal the batched form's, witnesses replay,
+    and the latency percentiles are ordered."""
+    perms, n, inst = _requests(td, 20000, seed=7)
+    maxd = n // 2 + 1
+    td.init_slots(1, [0], 64 << 20)
+    try:
+        res, st = td._lib.percall_open_loop(0, inst, 50000.0, clients=8, seed=11)
+        batch, _ = td.search_batch(0, inst, 0)
+    finally:
+        td.destroy()
+    assert st["served"] == 20000 and st["max_inflight"] == 8 and st["workers"] > 0
+    assert 0 < st["p50_ms"] <= st["p99_ms"] <= st["p999_ms"] <= st["max_ms"]
+    assert (res["status"] == batch["status"]).all()
+    _replays(oracle, td, perms, n, res, maxd)
