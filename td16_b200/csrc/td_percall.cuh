@@ -252,15 +252,17 @@ int percall_submit(PercallDevice &pd, int device, const td_instance &x, PercallS
                    unsigned long long *out_ticket, unsigned *out_gen, char *err, size_t errlen) {
     TD_CHECK(cudaSetDevice(device));
     PercallServer *ps = &pd.srv[pd.cur];
-    if (ps->running && cudaStreamQuery(ps->stream) != cudaErrorNotReady) {
-        // the launch has ended (idle, its deadline, or an error): start afresh
+    // the launch has ended (idle or its deadline; its dispatcher says so in
+    // mapped memory, so no CUDA call is needed to see it): start afresh.  A
+    // launch that failed is seen by its clients' own checks.
+    if (ps->running && __atomic_load_n(&ps->h_ctl->exit_reason, __ATOMIC_ACQUIRE) != 0) {
         cudaStreamSynchronize(ps->stream);
         ps->running = false;
         ps->retiring = false;
     }
     if (ps->running && std::chrono::steady_clock::now() - ps->started > percall_rotate_after()) {
         PercallServer &next = pd.srv[1 - pd.cur];
-        if (next.running && cudaStreamQuery(next.stream) != cudaErrorNotReady) {
+        if (next.running && __atomic_load_n(&next.h_ctl->exit_reason, __ATOMIC_ACQUIRE) != 0) {
             cudaStreamSynchronize(next.stream);
             next.running = false;
             next.retiring = false;

@@ -51,6 +51,12 @@ __device__ __forceinline__ void td_serve_record(td_serve_dev_ctl *dctl, const td
     atomicCAS(&dctl->error, 0, TD_ERR_TIMEOUT);
 }
 
+// Longest sleep of a polling warp between two polls (ns): the dispatcher
+// waiting for requests and the workers waiting for work.
+#ifndef TD_SERVE_BACKOFF_CAP
+#define TD_SERVE_BACKOFF_CAP 2048u
+#endif
+
 // Move order of a serving launch: every request in the free order, every
 // request in the reference order, or per request (TD_PACKED_ORDERED in the
 // request's packed byte; the per-call server of td_search and
@@ -136,7 +142,7 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
                 break;
             }
             __nanosleep(backoff);
-            backoff = min(backoff * 2u, 2048u);
+            backoff = min(backoff * 2u, (unsigned)TD_SERVE_BACKOFF_CAP);
         }
         return;
     }
@@ -208,7 +214,7 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
             }
             if (__shfl_sync(TD_FULL, stop, 0)) break;
             __nanosleep(backoff);
-            backoff = min(backoff * 2u, 2048u);
+            backoff = min(backoff * 2u, (unsigned)TD_SERVE_BACKOFF_CAP);
             continue;
         }
         if (lane == 0 && idle) { atomicSub(&pool->idle, 1); idle = false; }
