@@ -206,6 +206,56 @@ int td_search_pairs(int slot, int count, const uint8_t *beta, const uint8_t *ome
                     int32_t *status, int32_t *depth, int16_t *out_ijk, char *err,
                     size_t errlen);
 
+/* ---- pair consumer: the enumerator's Consumer<CyclicTargetPair> --------- */
+
+/* A thread-safe consumer that many producer threads feed one pair at a time
+ * (DirectTwistedBraceletGenerator.java:105-156 calls its consumer from every
+ * generator thread) and that searches the pairs in batches: one worker thread
+ * per slot (slots first_slot .. first_slot + slots - 1) takes a full batch
+ * and searches it with one call of `search` (td_search_pairs when NULL; any
+ * function of its signature, e.g. a test double).  A batch is handed over when
+ * it holds batch_size pairs, when its oldest pair has waited max_delay_s and a
+ * worker is idle (while all are busy it keeps filling), at td_batcher_flush,
+ * or at close.  td_batcher_accept blocks while max_pending
+ * full batches wait for a worker (0 = 2 x slots), as the reference's bounded
+ * queue of slots + tdp.gpuQueueCapacity jobs does (GPUSortingSearch.java:46-52).
+ * Results: found witnesses go to cert_writer (a td_cert_writer_open handle, or
+ * NULL), and done (or NULL) receives every searched batch on a worker thread:
+ * the tags given to accept, and per pair the status, depth and position
+ * triples td_search_pairs returns.  Batches complete in any order. */
+typedef void (*td_batcher_done_fn)(void *user, int count, const uint64_t *tags,
+                                   const int32_t *status, const int32_t *depth,
+                                   const int16_t *out_ijk);
+
+typedef int (*td_batcher_search_fn)(int slot, int count, const uint8_t *beta,
+                                    const uint8_t *omega, const uint8_t *n,
+                                    const int32_t *init, const float *min_rate,
+                                    const int32_t *max_moves, const uint8_t *full,
+                                    unsigned flags, int32_t *status, int32_t *depth,
+                                    int16_t *out_ijk, char *err, size_t errlen);
+
+typedef struct td_batcher_stats {
+    uint64_t pairs, batches, found, not_found, errors, certificates;
+    double search_s;  /* summed over workers: time inside td_search_pairs */
+} td_batcher_stats;
+
+int td_batcher_open(int first_slot, int slots, int batch_size, double max_delay_s,
+                    int max_pending, unsigned flags, td_batcher_search_fn search,
+                    void *cert_writer, td_batcher_done_fn done, void *user,
+                    void **handle, char *err, size_t errlen);
+/* Copies the pair (n <= 17 bytes each of beta and omega); TD_INVALID_ARG for
+ * a null handle or pointer or n > 17.  Per-pair errors (bad max_moves, ...)
+ * come back as that pair's status. */
+int td_batcher_accept(void *handle, uint64_t tag, const uint8_t *beta,
+                      const uint8_t *omega, int n, int initial_even_cycles,
+                      float min_rate, int max_moves, int full_sorting);
+int td_batcher_flush(void *handle);
+/* Hands over the filling batch, waits for every batch to be searched and
+ * delivered, and frees the consumer.  Returns TD_OK, or the first error of a
+ * whole batch call (its message in err). */
+int td_batcher_close(void *handle, td_batcher_stats *stats, char *err,
+                     size_t errlen);
+
 /* Device buffers; enqueues on `stream` (a cudaStream_t, or NULL for the
  * slot's stream) and returns without waiting. */
 int td_search_batch_device(int slot, int count, const td_instance *d_instances,

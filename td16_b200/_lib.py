@@ -41,6 +41,24 @@ class ServeStats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class BatcherStats(C.Structure):
+    _fields_ = [(name, C.c_uint64) for name in ("pairs", "batches", "found", "not_found", "errors",
+                                                 "certificates")] + [("search_s", C.c_double)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+# td_batcher_done_fn: (user, count, tags, status, depth, out_ijk)
+BATCHER_DONE = C.CFUNCTYPE(None, C.c_void_p, C.c_int, C.POINTER(C.c_uint64), C.POINTER(C.c_int32),
+                           C.POINTER(C.c_int32), C.POINTER(C.c_int16))
+
+
+# td_batcher_search_fn: td_search_pairs' signature
+BATCHER_SEARCH = C.CFUNCTYPE(C.c_int, C.c_int, C.c_int, *([C.c_void_p] * 7), C.c_uint, *([C.c_void_p] * 3),
+                             C.c_void_p, C.c_size_t)
+
+
 class TdError(RuntimeError):
     def __init__(self, code: int, message: str):
         super().__init__(message)
@@ -57,7 +75,8 @@ EXPORTS = ["td_init_slots", "td_search", "td_search_ordered", "td_slot_count", "
            "td_codec_key", "td_codec_value", "td_codec_decode_key", "td_codec_decode_value",
            "td_replay_symbols_device", "td_cert_writer_open", "td_cert_writer_enqueue", "td_cert_writer_close",
            "td_serve_open", "td_serve_workers", "td_serve_submit", "td_serve_poll", "td_serve_close",
-           "td_serve_open_loop", "td_configure_percall", "td_search_pairs", "td_percall_open_loop", "td_cert_writer_enqueue_batch", "td_cert_read_file", "td_pairs_from_perms", "td_batch_graph_create", "td_batch_graph_launch", "td_batch_graph_destroy"]
+           "td_serve_open_loop", "td_configure_percall", "td_search_pairs", "td_percall_open_loop", "td_cert_writer_enqueue_batch", "td_cert_read_file", "td_pairs_from_perms", "td_batch_graph_create", "td_batch_graph_launch", "td_batch_graph_destroy",
+           "td_batcher_open", "td_batcher_accept", "td_batcher_flush", "td_batcher_close"]
 
 
 def lib():
@@ -123,6 +142,11 @@ def lib():
     L.td_serve_close.argtypes = [vp, cp, sz]
     L.td_serve_open_loop.argtypes = [C.c_int, vp, C.c_int, C.c_double, C.c_uint64, C.c_uint64, C.c_uint, vp,
                                      C.POINTER(ServeStats), cp, sz]
+    L.td_batcher_open.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_uint, BATCHER_SEARCH, vp,
+                                  BATCHER_DONE, vp, C.POINTER(vp), cp, sz]
+    L.td_batcher_accept.argtypes = [vp, C.c_uint64, vp, vp, C.c_int, C.c_int, C.c_float, C.c_int, C.c_int]
+    L.td_batcher_flush.argtypes = [vp]
+    L.td_batcher_close.argtypes = [vp, C.POINTER(BatcherStats), cp, sz]
     _lib = L
     return L
 
@@ -486,6 +510,8 @@ def _threads_lib():
         h.td_slot_threads_run.restype = C.c_double
         h.td_slot_threads_run.argtypes = [C.c_int, C.c_void_p, C.c_int] + [C.c_void_p] * 7 + [
             C.c_int, C.c_int] + [C.c_void_p] * 5
+        h.td_producer_threads_run.restype = C.c_double
+        h.td_producer_threads_run.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 8
         _threads = h
     return _threads
 
@@ -518,3 +544,82 @@ def slot_threads_run(fn, beta, omega, n, init, rate, maxd, full, threads: int, f
 def entry_address(name: str) -> int:
     """Address of an entry point of the engine library (for slot_threads_run)."""
     return C.cast(getattr(lib(), name), C.c_void_p).value
+
+
+# ---- native pair consumer (td_batcher.cc) ---------------------------------------
+
+
+class PairConsumer:
+    """The enumerator's Consumer<CyclicTargetPair> in native code (td_batcher_*):
+    producers hand pairs over one at a time with `accept`; one native worker
+    per slot searches them in batches of `batch_size` (or whatever has waited
+    `max_delay_s`).  Found witnesses go to `cert_writer` (a CertificateWriter)
+    when given; `on_batch(tags, status, depth, moves)` receives each searched
+    batch as arrays (copies) when given.  `accept` blocks while `max_pending`
+    full batches wait (0: twice the slots).  `search` (a BATCHER_SEARCH
+    callable) replaces td_search_pairs; the CPU tests use it."""
+
+    def __init__(self, first_slot: int, slots: int, batch_size: int = 65536, max_delay_s: float = 0.002,
+                 max_pending: int = 0, ordered: bool = False, cert_writer=None, on_batch=None, search=None):
+        self._on_batch = on_batch
+        self._cb = BATCHER_DONE(self._deliver) if on_batch is not None else BATCHER_DONE()
+        self._search = search if search is not None else BATCHER_SEARCH()
+        self._h = C.c_void_p()
+        err = C.create_string_buffer(512)
+        rc = lib().td_batcher_open(int(first_slot), int(slots), int(batch_size), float(max_delay_s), int(max_pending),
+                                   FLAG_ORDERED if ordered else 0, self._search,
+                                   cert_writer._h if cert_writer is not None else None, self._cb, None,
+                                   C.byref(self._h), err, 512)
+        check(rc, err)
+        self.stats = None
+
+    def _deliver(self, _user, count, tags, status, depth, ijk):
+        t = np.ctypeslib.as_array(tags, (count,)).copy()
+        st = np.ctypeslib.as_array(status, (count,)).copy()
+        d = np.ctypeslib.as_array(depth, (count,)).copy()
+        m = np.ctypeslib.as_array(ijk, (count * 27,)).reshape(count, 9, 3).copy()
+        self._on_batch(t, st, d, m)
+
+    @property
+    def handle(self):
+        return self._h.value
+
+    def accept(self, tag: int, beta, omega, initial_even_cycles: int, min_rate: float, max_moves: int,
+               full_sorting: bool = True) -> None:
+        beta, omega = bytes(beta), bytes(omega)
+        if len(beta) != len(omega):
+            raise TdError(INVALID_ARG, "beta and omega must have equal lengths")
+        rc = lib().td_batcher_accept(self._h, int(tag), beta, omega, len(beta), int(initial_even_cycles),
+                                     float(min_rate), int(max_moves), int(bool(full_sorting)))
+        check(rc, None)
+
+    def flush(self) -> None:
+        lib().td_batcher_flush(self._h)
+
+    def close(self) -> dict:
+        if self._h:
+            st = BatcherStats()
+            err = C.create_string_buffer(512)
+            rc = lib().td_batcher_close(self._h, C.byref(st), err, 512)
+            self._h = C.c_void_p()
+            self.stats = st.as_dict()
+            check(rc, err)
+        return self.stats
+
+
+def producer_threads_run(consumer: PairConsumer, threads: int, beta, omega, n, init, rate, maxd, full=1) -> float:
+    """Hands `count` pairs to `consumer` from `threads` native producer threads
+    (thread t: pairs t, t + threads, ..., tagged with their index).  Returns
+    the producers' wall time in seconds."""
+    count = int(beta.shape[0])
+    beta = np.ascontiguousarray(beta, np.uint8)
+    omega = np.ascontiguousarray(omega, np.uint8)
+    bc = lambda v, dt: np.ascontiguousarray(np.broadcast_to(v, (count,)), dt)  # noqa: E731
+    arrs = [bc(n, np.int32), bc(init, np.int32), bc(rate, np.float32), bc(maxd, np.int32), bc(full, np.uint8)]
+    first = np.zeros(1, np.int32)
+    secs = _threads_lib().td_producer_threads_run(C.c_void_p(entry_address("td_batcher_accept")), consumer.handle,
+                                                  int(threads), count, _ptr(beta), _ptr(omega),
+                                                  *[_ptr(a) for a in arrs], _ptr(first))
+    if first[0] != OK:
+        raise TdError(int(first[0]), f"a producer's accept returned {int(first[0])}")
+    return secs

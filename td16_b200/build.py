@@ -27,11 +27,11 @@ def nvcc() -> str:
 
 
 def _sources():
-    return [os.path.join(CSRC, "td_engine.cu"), os.path.join(CSRC, "td_cert.cu")]
+    return [os.path.join(CSRC, "td_engine.cu"), os.path.join(CSRC, "td_cert.cu"), os.path.join(CSRC, "td_batcher.cc")]
 
 
 def _deps():
-    return [p for p in glob.glob(os.path.join(CSRC, "*")) if p.endswith((".cu", ".cuh"))] + [
+    return [p for p in glob.glob(os.path.join(CSRC, "*")) if p.endswith((".cu", ".cuh", "td_batcher.cc"))] + [
         os.path.join(PKG, "..", "include", "td16_b200.h")]
 
 
@@ -44,7 +44,8 @@ def up_to_date(target: str, deps=None) -> bool:
 
 def build(verbose: bool = False, force: bool = False) -> str:
     if force or not up_to_date(LIB):
-        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-I", CSRC, "-o", LIB, *_sources(), "-lcudart"]
+        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-I", CSRC, "-I", os.path.join(PKG, "..", "include"), "-o", LIB,
+               *_sources(), "-lcudart"]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         res = subprocess.run(cmd, capture_output=True, text=True)

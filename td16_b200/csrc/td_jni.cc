@@ -6,6 +6,11 @@
 //                                    emitter/src/native/jni/jni_sorter.cu:24-117)
 //   searchForSortingSeqBatch         an addition for a case producer that
 //                                    hands over pairs in groups
+//   openPairConsumer, acceptPair,    an addition for the enumerator's
+//   closePairConsumer                Consumer<CyclicTargetPair>: pairs handed
+//                                    over one per call, searched in batches by
+//                                    the native consumer (td_batcher_*), found
+//                                    witnesses written as certificates
 // A non-OK status becomes a java.lang.RuntimeException carrying the engine's
 // message, as jni_sorter.cu:15-22,111-115 does for every C++ exception.  Built
 // only where a JDK's jni.h exists (td16_b200/build.py); the tests compile it
@@ -183,4 +188,108 @@ extern "C" JNIEXPORT jobjectArray JNICALL Java_br_unb_cic_tdp_base_GPUSortingSea
     }
     env->DeleteLocalRef(moves_class);
     return outer;
+}
+
+// ---- the native pair consumer ---------------------------------------------
+
+namespace {
+struct JniPairConsumer {
+    void *batcher;
+    void *writer;  // certificate file, or null
+};
+}  // namespace
+
+// Opens a consumer whose `slots` workers (slots firstSlot ..) search batches
+// of batchSize pairs (or what has waited maxDelaySeconds); at most maxPending
+// full batches wait (0: twice the slots) before acceptPair blocks.  With a
+// certificatePath, found witnesses are written there as certificate records
+// (the codec's bytes).  Returns the handle for acceptPair / closePairConsumer.
+extern "C" JNIEXPORT jlong JNICALL Java_br_unb_cic_tdp_base_GPUSortingSearch_openPairConsumer(
+    JNIEnv *env, jclass, jint first_slot, jint slots, jint batch_size, jdouble max_delay_s, jint max_pending,
+    jstring certificate_path) {
+    void *writer = nullptr;
+    if (certificate_path != nullptr) {
+        const char *path = env->GetStringUTFChars(certificate_path, nullptr);
+        if (path == nullptr) return 0;  // the JVM has raised OutOfMemoryError
+        writer = td_cert_writer_open(path, 5.0);
+        env->ReleaseStringUTFChars(certificate_path, path);
+        if (writer == nullptr) {
+            throw_runtime(env, "cannot open the certificate file");
+            return 0;
+        }
+    }
+    void *h = nullptr;
+    char err[512] = {0};
+    const int rc = td_batcher_open((int)first_slot, (int)slots, (int)batch_size, (double)max_delay_s,
+                                   (int)max_pending, 0u, nullptr, writer, nullptr, nullptr, &h, err, sizeof err);
+    if (rc != TD_OK) {
+        if (writer) td_cert_writer_close(writer);
+        throw_runtime(env, err[0] ? err : "openPairConsumer failed");
+        return 0;
+    }
+    return reinterpret_cast<jlong>(new JniPairConsumer{h, writer});
+}
+
+// Hands one pair to the consumer (blocks while its queue is full).  `tag`
+// identifies the pair in the consumer's statistics and callbacks.
+extern "C" JNIEXPORT void JNICALL Java_br_unb_cic_tdp_base_GPUSortingSearch_acceptPair(
+    JNIEnv *env, jclass, jlong handle, jlong tag, jbyteArray beta, jbyteArray omega, jint initial_even_cycles,
+    jfloat min_rate, jint max_moves, jboolean full_sorting) {
+    auto *c = reinterpret_cast<JniPairConsumer *>(handle);
+    if (c == nullptr) {
+        throw_runtime(env, "the pair consumer is not open");
+        return;
+    }
+    if (beta == nullptr || omega == nullptr) {
+        throw_runtime(env, "beta and omega must not be null");
+        return;
+    }
+    const jsize n = env->GetArrayLength(beta);
+    if (env->GetArrayLength(omega) != n) {
+        throw_runtime(env, "beta and omega must have equal lengths");
+        return;
+    }
+    if (n > 17) {
+        throw_runtime(env, "performGpuSortingSearch: n exceeds MAX_N");
+        return;
+    }
+    uint8_t b[17], o[17];
+    if (n > 0) {
+        env->GetByteArrayRegion(beta, 0, n, reinterpret_cast<jbyte *>(b));
+        env->GetByteArrayRegion(omega, 0, n, reinterpret_cast<jbyte *>(o));
+    }
+    const int rc = td_batcher_accept(c->batcher, (uint64_t)tag, b, o, (int)n, (int)initial_even_cycles,
+                                     (float)min_rate, (int)max_moves, full_sorting ? 1 : 0);
+    if (rc != TD_OK) throw_runtime(env, "the pair consumer rejected the pair");
+}
+
+// Searches what is left, closes the certificate file and frees the consumer.
+// Returns long[6]: pairs, batches, found, not found, errors (per-pair error
+// statuses), certificates written.  A batch call that failed (a CUDA error,
+// an invalid slot) raises RuntimeException with its message instead.
+extern "C" JNIEXPORT jlongArray JNICALL Java_br_unb_cic_tdp_base_GPUSortingSearch_closePairConsumer(
+    JNIEnv *env, jclass, jlong handle) {
+    auto *c = reinterpret_cast<JniPairConsumer *>(handle);
+    if (c == nullptr) {
+        throw_runtime(env, "the pair consumer is not open");
+        return nullptr;
+    }
+    td_batcher_stats st{};
+    char err[512] = {0};
+    const int rc = td_batcher_close(c->batcher, &st, err, sizeof err);
+    const long long written = c->writer ? td_cert_writer_close(c->writer) : 0;
+    delete c;
+    if (rc != TD_OK) {
+        throw_runtime(env, err[0] ? err : "GPU sorting search failed");
+        return nullptr;
+    }
+    if (written < 0) {
+        throw_runtime(env, "writing the certificate file failed");
+        return nullptr;
+    }
+    const jlong out[6] = {(jlong)st.pairs, (jlong)st.batches, (jlong)st.found, (jlong)st.not_found,
+                          (jlong)st.errors, (jlong)written};
+    jlongArray arr = env->NewLongArray(6);
+    env->SetLongArrayRegion(arr, 0, 6, out);
+    return arr;
 }

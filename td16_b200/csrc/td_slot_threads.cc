@@ -1,7 +1,9 @@
 // td_slot_threads.cc -- drives a blocking search entry point from native host
 // threads, one thread per slot, the way the emitter's Java slot workers call
 // searchForSortingSeq (GPUSortingSearch.java:134-147: one worker thread per
-// slot, each taking the next queued case and blocking in the native call).
+// slot, each taking the next queued case and blocking in the native call);
+// and feeds a pair consumer from native producer threads, the way the
+// enumerator's generator threads call theirs (td_producer_threads_run).
 //
 // Built as libtd16_slot_threads.so.  It links nothing: the search entry point
 // is passed as a function pointer, so the same driver runs this engine's
@@ -73,5 +75,44 @@ extern "C" __attribute__((visibility("default"))) double td_slot_threads_run(
     std::vector<std::thread> th;
     for (int t = 0; t < threads; ++t) th.emplace_back(worker, first_slot + t);
     for (auto &t : th) t.join();
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+namespace {
+
+// td_batcher_accept's signature
+typedef int (*pair_accept_fn)(void *handle, uint64_t tag, const uint8_t *beta, const uint8_t *omega, int n,
+                              int init, float rate, int maxd, int full);
+
+}  // namespace
+
+// Feeds `count` pairs to a pair consumer from `threads` native producer
+// threads, the way the enumerator's generator threads call their consumer
+// (DirectTwistedBraceletGenerator.java:105-156): thread t hands over pairs t,
+// t + threads, ... one call each, with the pair's index as its tag.  `fn` has
+// td_batcher_accept's signature.  *first_rc receives the first non-zero
+// return code (0 when every call succeeded).  Returns the producers' wall
+// time in seconds.
+extern "C" __attribute__((visibility("default"))) double td_producer_threads_run(
+    void *fn, void *handle, int threads, int count, const uint8_t *beta, const uint8_t *omega, const int32_t *n,
+    const int32_t *init, const float *rate, const int32_t *maxd, const uint8_t *full, int32_t *first_rc) {
+    std::atomic<int> rc_seen{0};
+    auto producer = [&](int t) {
+        for (int i = t; i < count; i += threads) {
+            const int rc = reinterpret_cast<pair_accept_fn>(fn)(handle, (uint64_t)i, beta + 17 * (size_t)i,
+                                                                omega + 17 * (size_t)i, n[i], init[i], rate[i],
+                                                                maxd[i], full[i]);
+            if (rc != 0) {
+                int expect = 0;
+                rc_seen.compare_exchange_strong(expect, rc);
+                return;
+            }
+        }
+    };
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::thread> th;
+    for (int t = 0; t < threads; ++t) th.emplace_back(producer, t);
+    for (auto &t : th) t.join();
+    if (first_rc) *first_rc = rc_seen.load();
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }

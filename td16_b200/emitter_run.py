@@ -9,7 +9,7 @@ witness, and hand the witnesses to the certificate sink in the reference's
 byte format (CertificateCodec).  Afterwards every stored record is read back
 and replayed on the GPU with the checker's rules.
 
-Three shapes of the host side (--mode):
+Four shapes of the host side (--mode):
   batch     a slot thread searches a batch of cases per call (td_search_batch)
   percall   the reference's shape: one blocking td_search per case from
             `slots` native threads, one per slot (GPUSortingSearch.java:134-162)
@@ -17,6 +17,9 @@ Three shapes of the host side (--mode):
             time to a thread-safe consumer (DirectTwistedBraceletGenerator.
             generateRepresentativesConcurrently), here host.PairBatcher, which
             searches them in batches with td_search_pairs
+  native    the same shape in native code: producer threads hand cases one at
+            a time to the native pair consumer (td_batcher_*), whose slot
+            workers search batches and write the certificates themselves
 
     python -m td16_b200.emitter_run [--mode batch] [--count N] [--slots 16]
                                     [--budget-gib 4] [--batch 65536] [--out certs.bin]
@@ -176,6 +179,34 @@ def run_consumer(count: int, slots: int, budget: int, out_path: str, seed: int =
             "witnesses_per_s": written / wall, "replay": rep}
 
 
+def run_native_consumer(count: int, slots: int, budget: int, out_path: str, seed: int = 4, device: int = 0,
+                        producers: int = 16, batch: int = 65536) -> dict:
+    """Native producer threads hand cases one at a time to the native pair
+    consumer (td_batcher_accept); its slot workers search batches and pass
+    the witnesses straight to the certificate writer."""
+    _lib.init_slots(slots, [device], budget)
+    if os.path.exists(out_path):
+        os.remove(out_path)
+    perms, n = _chunk(seed, 0, count)
+    beta, omega = _pairs(perms, n)
+    init = (_lib.prepare_perms(perms, n, 9)["packed"] & 31).astype(np.int32)
+    writer = _lib.CertificateWriter(out_path, 5.0)
+    t0 = time.perf_counter()
+    cons = _lib.PairConsumer(0, slots, batch_size=batch, max_delay_s=0.005, cert_writer=writer)
+    try:
+        produce_s = _lib.producer_threads_run(cons, producers, beta, omega, 17, init, 0.0, 9)
+    finally:
+        stats = cons.close()
+    written = writer.close()
+    wall = time.perf_counter() - t0
+    _lib.destroy()
+    rep = replay_file(out_path, 17)
+    return {"mode": "native", "cases": count, "slots": slots, "producers": producers, "batch": batch,
+            "batches": stats["batches"], "found": stats["found"], "not_found": stats["not_found"],
+            "errors": stats["errors"], "certificates": written, "wall_s": wall, "produce_s": produce_s,
+            "search_s_summed": stats["search_s"], "witnesses_per_s": written / wall, "replay": rep}
+
+
 def run(count: int, slots: int, budget: int, batch: int, out_path: str, seed: int = 4, device: int = 0) -> dict:
     _lib.init_slots(slots, [device], budget)
     if os.path.exists(out_path):
@@ -241,13 +272,15 @@ def main():
     ap.add_argument("--batch", type=int, default=65536)
     ap.add_argument("--out", default="certs.bin")
     ap.add_argument("--seed", type=int, default=4)
-    ap.add_argument("--mode", default="batch", choices=["batch", "percall", "consumer"])
+    ap.add_argument("--mode", default="batch", choices=["batch", "percall", "consumer", "native"])
     a = ap.parse_args()
     budget = int(a.budget_gib * (1 << 30))
     if a.mode == "percall":
         out = run_percall(a.count, a.slots, budget, a.out, a.seed)
     elif a.mode == "consumer":
         out = run_consumer(a.count, a.slots, budget, a.out, a.seed)
+    elif a.mode == "native":
+        out = run_native_consumer(a.count, a.slots, budget, a.out, a.seed, batch=a.batch)
     else:
         out = run(a.count, a.slots, budget, a.batch, a.out, a.seed)
     print(json.dumps(out))

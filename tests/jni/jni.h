@@ -23,6 +23,7 @@ typedef int64_t jlong;
 typedef int8_t jbyte;
 typedef uint8_t jboolean;
 typedef float jfloat;
+typedef double jdouble;
 typedef jint jsize;
 
 class _jobject {};
@@ -34,6 +35,8 @@ class _jbyteArray : public _jarray {};
 class _jintArray : public _jarray {};
 class _jfloatArray : public _jarray {};
 class _jbooleanArray : public _jarray {};
+class _jlongArray : public _jarray {};
+class _jstring : public _jobject {};
 
 typedef _jobject *jobject;
 typedef _jclass *jclass;
@@ -44,6 +47,8 @@ typedef _jbyteArray *jbyteArray;
 typedef _jintArray *jintArray;
 typedef _jfloatArray *jfloatArray;
 typedef _jbooleanArray *jbooleanArray;
+typedef _jlongArray *jlongArray;
+typedef _jstring *jstring;
 
 struct JNIEnv_;
 
@@ -64,6 +69,10 @@ struct TestJniFunctions {
     void (*SetIntArrayRegion)(JNIEnv_ *, jintArray, jsize, jsize, const jint *);
     jobject (*GetObjectArrayElement)(JNIEnv_ *, jobjectArray, jsize);
     void (*SetObjectArrayElement)(JNIEnv_ *, jobjectArray, jsize, jobject);
+    const char *(*GetStringUTFChars)(JNIEnv_ *, jstring, jboolean *);
+    void (*ReleaseStringUTFChars)(JNIEnv_ *, jstring, const char *);
+    jlongArray (*NewLongArray)(JNIEnv_ *, jsize);
+    void (*SetLongArrayRegion)(JNIEnv_ *, jlongArray, jsize, jsize, const jlong *);
 };
 
 struct JNIEnv_ {
@@ -85,6 +94,10 @@ struct JNIEnv_ {
     void SetIntArrayRegion(jintArray a, jsize s, jsize l, const jint *b) { functions->SetIntArrayRegion(this, a, s, l, b); }
     jobject GetObjectArrayElement(jobjectArray a, jsize i) { return functions->GetObjectArrayElement(this, a, i); }
     void SetObjectArrayElement(jobjectArray a, jsize i, jobject v) { functions->SetObjectArrayElement(this, a, i, v); }
+    const char *GetStringUTFChars(jstring s, jboolean *copy) { return functions->GetStringUTFChars(this, s, copy); }
+    void ReleaseStringUTFChars(jstring s, const char *c) { functions->ReleaseStringUTFChars(this, s, c); }
+    jlongArray NewLongArray(jsize n) { return functions->NewLongArray(this, n); }
+    void SetLongArrayRegion(jlongArray a, jsize s, jsize l, const jlong *b) { functions->SetLongArrayRegion(this, a, s, l, b); }
 };
 typedef JNIEnv_ JNIEnv;
 

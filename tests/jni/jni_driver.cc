@@ -10,13 +10,17 @@
 //   real-cpu  linked to libtd16b200.so on a machine without a GPU: argument
 //             checks and initialisation failures
 //   real-gpu  linked to libtd16b200.so with a B200: real searches, every
-//             witness replayed, batch and per-call natives agreeing
+//             witness replayed, batch, per-call and pair-consumer natives
+//             agreeing
 // Prints one line per failed check and "jni ok <checks>" at the end; exits 1
 // on any failure.
 #include <jni.h>
 
+#include <unistd.h>
+
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <random>
 #include <string>
@@ -30,6 +34,11 @@ JNIEXPORT jobjectArray JNICALL Java_br_unb_cic_tdp_base_GPUSortingSearch_searchF
     JNIEnv *, jclass, jbyteArray, jbyteArray, jint, jfloat, jint, jboolean, jint);
 JNIEXPORT jobjectArray JNICALL Java_br_unb_cic_tdp_base_GPUSortingSearch_searchForSortingSeqBatch(
     JNIEnv *, jclass, jobjectArray, jobjectArray, jintArray, jfloatArray, jintArray, jbooleanArray, jint);
+JNIEXPORT jlong JNICALL Java_br_unb_cic_tdp_base_GPUSortingSearch_openPairConsumer(JNIEnv *, jclass, jint, jint, jint,
+                                                                                   jdouble, jint, jstring);
+JNIEXPORT void JNICALL Java_br_unb_cic_tdp_base_GPUSortingSearch_acceptPair(JNIEnv *, jclass, jlong, jlong, jbyteArray,
+                                                                            jbyteArray, jint, jfloat, jint, jboolean);
+JNIEXPORT jlongArray JNICALL Java_br_unb_cic_tdp_base_GPUSortingSearch_closePairConsumer(JNIEnv *, jclass, jlong);
 }
 
 namespace {
@@ -37,13 +46,14 @@ namespace {
 // ---- the fake JVM side --------------------------------------------------------
 
 struct Obj {
-    enum Kind { CLASS, BYTES, INTS, FLOATS, BOOLS, OBJECTS } kind;
-    std::string name;  // class name, or the element class of an object array
+    enum Kind { CLASS, BYTES, INTS, FLOATS, BOOLS, OBJECTS, STRING, LONGS } kind;
+    std::string name;  // class name, the element class of an object array, or a string's text
     std::vector<jbyte> b;
     std::vector<jint> i;
     std::vector<jfloat> f;
     std::vector<jboolean> z;
     std::vector<jobject> o;
+    std::vector<jlong> l;
 };
 
 std::vector<Obj *> g_heap;
@@ -90,6 +100,7 @@ jsize f_array_length(JNIEnv *, jarray a) {
         case Obj::FLOATS: return (jsize)o->f.size();
         case Obj::BOOLS: return (jsize)o->z.size();
         case Obj::OBJECTS: return (jsize)o->o.size();
+        case Obj::LONGS: return (jsize)o->l.size();
         default: return 0;
     }
 }
@@ -126,11 +137,27 @@ jobject f_get_element(JNIEnv *, jobjectArray a, jsize i) {
 void f_set_element(JNIEnv *, jobjectArray a, jsize i, jobject v) {
     if (in_range(get(a)->o, i, 1)) get(a)->o[i] = v;
 }
+int g_strings_held = 0;
+const char *f_get_string_utf(JNIEnv *, jstring str, jboolean *copy) {
+    if (copy) *copy = 0;
+    ++g_strings_held;
+    return get(str)->name.c_str();
+}
+void f_release_string_utf(JNIEnv *, jstring, const char *) { --g_strings_held; }
+jlongArray f_new_long_array(JNIEnv *, jsize n) {
+    Obj *o = new Obj{Obj::LONGS, "[J"};
+    o->l.assign(n, 0);
+    return make<jlongArray>(o);
+}
+void f_set_longs(JNIEnv *, jlongArray a, jsize s, jsize l, const jlong *in) {
+    if (in_range(get(a)->l, s, l)) std::memcpy(get(a)->l.data() + s, in, sizeof(jlong) * l);
+}
 
 const TestJniFunctions kFunctions = {f_exception_check, f_exception_clear, f_find_class,   f_throw_new,
                                      f_delete_local_ref, f_array_length,  f_get_bytes,    f_get_ints,
                                      f_get_floats,      f_get_bools,      f_new_object_array, f_new_int_array,
-                                     f_set_ints,        f_get_element,    f_set_element};
+                                     f_set_ints,        f_get_element,    f_set_element,
+                                     f_get_string_utf,  f_release_string_utf, f_new_long_array, f_set_longs};
 JNIEnv g_env{&kFunctions};
 
 jbyteArray bytes(std::vector<int> v) {
@@ -153,6 +180,8 @@ jbooleanArray bools(std::vector<jboolean> v) {
     o->z = v;
     return make<jbooleanArray>(o);
 }
+jstring jstr(const std::string &text) { return make<jstring>(new Obj{Obj::STRING, text}); }
+std::vector<jlong> longs_of(jlongArray a) { return get(a)->l; }
 jobjectArray byte_rows(const std::vector<std::vector<int>> &rows) {
     Obj *o = new Obj{Obj::OBJECTS, "[B"};
     for (auto &r : rows) o->o.push_back(reinterpret_cast<jobject>(bytes(r)));
@@ -296,6 +325,121 @@ extern "C" int td_search_pairs(int slot, int count, const uint8_t *, const uint8
     return TD_OK;
 }
 
+// the pair consumer and certificate writer, recorded
+static int g_open_rc = TD_OK, g_accept_rc = TD_OK, g_close_rc = TD_OK;
+static std::string g_open_msg, g_close_msg, g_seen_path;
+static int g_seen_open[5];
+static double g_seen_delay = 0;
+static void *g_seen_writer = nullptr;
+static bool g_writer_null = false, g_writer_closed = false, g_batcher_closed = false;
+static long long g_writer_written = 0;
+static uint64_t g_seen_tag = 0;
+static td_batcher_stats g_next_stats{};
+static int g_writer_token, g_batcher_token;
+
+extern "C" void *td_cert_writer_open(const char *path, double) {
+    g_seen_path = path;
+    g_writer_closed = false;
+    return g_writer_null ? nullptr : &g_writer_token;
+}
+extern "C" long long td_cert_writer_close(void *w) {
+    g_writer_closed = w == &g_writer_token;
+    return g_writer_written;
+}
+extern "C" int td_batcher_open(int first_slot, int slots, int batch, double delay, int pending, unsigned,
+                               td_batcher_search_fn, void *writer, td_batcher_done_fn, void *, void **h, char *err,
+                               size_t errlen) {
+    const int seen[5] = {first_slot, slots, batch, pending, 0};
+    std::memcpy(g_seen_open, seen, sizeof seen);
+    g_seen_delay = delay;
+    g_seen_writer = writer;
+    g_batcher_closed = false;
+    if (g_open_rc != TD_OK) {
+        std::snprintf(err, errlen, "%s", g_open_msg.c_str());
+        return g_open_rc;
+    }
+    *h = &g_batcher_token;
+    return TD_OK;
+}
+extern "C" int td_batcher_accept(void *h, uint64_t tag, const uint8_t *beta, const uint8_t *, int n, int,
+                                 float rate, int maxd, int full) {
+    if (h != &g_batcher_token) return TD_INVALID_ARG;
+    g_seen_tag = tag;
+    g_seen_n = n;
+    g_seen_beta.assign(beta, beta + n);
+    g_seen_rate = rate;
+    g_seen_maxd = maxd;
+    g_seen_full = full;
+    return g_accept_rc;
+}
+extern "C" int td_batcher_close(void *h, td_batcher_stats *st, char *err, size_t errlen) {
+    g_batcher_closed = h == &g_batcher_token;
+    *st = g_next_stats;
+    if (g_close_rc != TD_OK) std::snprintf(err, errlen, "%s", g_close_msg.c_str());
+    return g_close_rc;
+}
+
+static void run_fake_consumer() {
+    auto open = [](jstring path) {
+        return Java_br_unb_cic_tdp_base_GPUSortingSearch_openPairConsumer(&g_env, nullptr, 2, 3, 128, 0.25, 5, path);
+    };
+    auto accept = [](jlong h, std::vector<int> beta, std::vector<int> omega) {
+        Java_br_unb_cic_tdp_base_GPUSortingSearch_acceptPair(&g_env, nullptr, h, 41, beta.empty() ? nullptr : bytes(beta),
+                                                             bytes(omega), 1, 1.7777778f, 8, false);
+    };
+    jlong h = open(nullptr);
+    check(h != 0 && !g_pending && g_seen_open[0] == 2 && g_seen_open[1] == 3 && g_seen_open[2] == 128 &&
+              g_seen_open[3] == 5 && g_seen_delay == 0.25 && g_seen_writer == nullptr,
+          "openPairConsumer passes its settings through, no writer without a path");
+    accept(h, {0, 200, 2}, {1, 2, 0});
+    check(!g_pending && g_seen_tag == 41 && g_seen_n == 3 && g_seen_beta[1] == 200 && g_seen_rate == 1.7777778f &&
+              g_seen_maxd == 8 && g_seen_full == 0,
+          "acceptPair passes tag, bytes unsigned, rate, depth and fullSorting");
+    accept(0, {0, 1, 2}, {1, 2, 0});
+    check(threw("the pair consumer is not open"), "acceptPair(0)");
+    accept(h, {}, {1, 2, 0});
+    check(threw("beta and omega must not be null"), "acceptPair(null beta)");
+    accept(h, {0, 1, 2}, {1, 2});
+    check(threw("beta and omega must have equal lengths"), "acceptPair(unequal lengths)");
+    accept(h, std::vector<int>(18, 0), std::vector<int>(18, 0));
+    check(threw("performGpuSortingSearch: n exceeds MAX_N"), "acceptPair(n > 17)");
+    g_accept_rc = TD_INVALID_ARG;
+    accept(h, {0, 1, 2}, {1, 2, 0});
+    check(threw("the pair consumer rejected the pair"), "acceptPair rejected");
+    g_accept_rc = TD_OK;
+    g_next_stats = td_batcher_stats{10, 2, 6, 3, 1, 6, 0.5};
+    jlongArray st = Java_br_unb_cic_tdp_base_GPUSortingSearch_closePairConsumer(&g_env, nullptr, h);
+    check(st && !g_pending && g_batcher_closed && longs_of(st) == std::vector<jlong>({10, 2, 6, 3, 1, 0}),
+          "closePairConsumer: long[6], no certificates without a writer");
+    check(Java_br_unb_cic_tdp_base_GPUSortingSearch_closePairConsumer(&g_env, nullptr, 0) == nullptr &&
+              threw("the pair consumer is not open"),
+          "closePairConsumer(0)");
+
+    h = open(jstr("/tmp/certs.bin"));
+    check(h != 0 && g_seen_path == "/tmp/certs.bin" && g_seen_writer == &g_writer_token && g_strings_held == 0,
+          "openPairConsumer with a path opens the certificate writer and releases the string");
+    g_writer_written = 6;
+    st = Java_br_unb_cic_tdp_base_GPUSortingSearch_closePairConsumer(&g_env, nullptr, h);
+    check(st && g_writer_closed && longs_of(st)[5] == 6, "closePairConsumer closes the writer and counts its records");
+    g_writer_written = 0;
+
+    g_writer_null = true;
+    check(open(jstr("/nonexistent/x")) == 0 && threw("cannot open the certificate file"), "unwritable path");
+    g_writer_null = false;
+    g_open_rc = TD_INVALID_ARG;
+    g_open_msg = "td_batcher_open: needs slots";
+    check(open(jstr("/tmp/c2.bin")) == 0 && threw("td_batcher_open: needs slots") && g_writer_closed,
+          "open failure raises and closes the writer");
+    g_open_rc = TD_OK;
+    h = open(nullptr);
+    g_close_rc = TD_CUDA_ERROR;
+    g_close_msg = "CUDA error";
+    check(Java_br_unb_cic_tdp_base_GPUSortingSearch_closePairConsumer(&g_env, nullptr, h) == nullptr &&
+              threw("CUDA error") && g_batcher_closed,
+          "a failed batch call raises at close");
+    g_close_rc = TD_OK;
+}
+
 static void run_fake() {
     auto init = [](jintArray devs, jlong budget) {
         Java_br_unb_cic_tdp_base_GPUSortingSearch_initSlots(&g_env, nullptr, 4, devs, budget);
@@ -380,6 +524,7 @@ static void run_fake() {
     g_next_msg = "CUDA error";
     check(batch(byte_rows({{0, 1, 2}}), byte_rows({{1, 2, 0}}), 1) == nullptr && threw("CUDA error"),
           "batch call error -> RuntimeException");
+    run_fake_consumer();
 }
 #else
 static void run_real(bool gpu) {
@@ -388,6 +533,14 @@ static void run_real(bool gpu) {
         check(threw_any(), "initSlots without a GPU raises");
         check(search({0, 1, 2}, {1, 2, 0}, 1, 2.0f, 1, true, 0) == nullptr && threw("invalid GPU sorting slot"),
               "search on an uninitialised slot");
+        const jlong h = Java_br_unb_cic_tdp_base_GPUSortingSearch_openPairConsumer(&g_env, nullptr, 0, 1, 8, 0.001, 0,
+                                                                                   nullptr);
+        check(h != 0 && !g_pending, "openPairConsumer without a GPU");
+        Java_br_unb_cic_tdp_base_GPUSortingSearch_acceptPair(&g_env, nullptr, h, 0, bytes({0, 1, 2}), bytes({1, 2, 0}),
+                                                             1, 2.0f, 1, true);
+        check(!g_pending, "acceptPair without a GPU");
+        check(Java_br_unb_cic_tdp_base_GPUSortingSearch_closePairConsumer(&g_env, nullptr, h) == nullptr && threw_any(),
+              "a batch on an uninitialised slot raises at close");
         return;
     }
     Java_br_unb_cic_tdp_base_GPUSortingSearch_initSlots(&g_env, nullptr, 2, ints({0}), 32 << 20);
@@ -438,6 +591,24 @@ static void run_real(bool gpu) {
         if (f) check(replays(betas[c], omegas[c], moves_of(row), maxds[c]), "batch replay " + std::to_string(c));
     }
     check(found > 0 && found < 96, "both verdicts occur");
+    // the same pairs through the native consumer, witnesses to a certificate file
+    char path[] = "/tmp/td_jni_certsXXXXXX";
+    const int fd = mkstemp(path);
+    check(fd >= 0, "temporary certificate file");
+    if (fd >= 0) close(fd);
+    const jlong h = Java_br_unb_cic_tdp_base_GPUSortingSearch_openPairConsumer(&g_env, nullptr, 0, 2, 32, 0.002, 0,
+                                                                               jstr(path));
+    check(h != 0 && !g_pending, "openPairConsumer(2 slots, batches of 32)");
+    for (int c = 0; h && c < 96; ++c)
+        Java_br_unb_cic_tdp_base_GPUSortingSearch_acceptPair(&g_env, nullptr, h, c, bytes(betas[c]), bytes(omegas[c]),
+                                                             inits[c], 0.f, maxds[c], true);
+    check(!g_pending, "acceptPair x 96");
+    jlongArray st = h ? Java_br_unb_cic_tdp_base_GPUSortingSearch_closePairConsumer(&g_env, nullptr, h) : nullptr;
+    check(st && !g_pending &&
+              longs_of(st) == std::vector<jlong>({96, longs_of(st)[1], found, 96 - found, 0, found}) &&
+              longs_of(st)[1] >= 3,
+          "consumer: every pair searched, the batch verdicts, one certificate per witness");
+    unlink(path);
     td_destroy();
 }
 #endif

@@ -4,9 +4,11 @@ fake JNIEnv (tests/jni/jni_driver.cc), the way GPUSortingSearch.java calls its
 natives (jni_sorter.cu:24-117 is the reference shim).
 
   fake engine   every engine status mapped to its RuntimeException, int[][]
-                shapes, argument pass-through, the batch native (no GPU)
+                shapes, argument pass-through, the batch native and the pair
+                consumer natives (no GPU)
   real engine   linked to libtd16b200.so: argument checks and initialisation
-                failure without a GPU; real searches with one
+                failure without a GPU; real searches with one, per call, in a
+                batch and through the pair consumer with its certificate file
 """
 import os
 import subprocess
