@@ -283,8 +283,15 @@ def serving_legs(td, device):
     try:
         out[f"clients_{clients}"] = sweep(lambda x, r: _lib.percall_open_loop(device, x, r, clients=clients, seed=5),
                                           rates[:5])
-        _, bst = td.search_batch(0, inst_s[:100000], 0)
-        out["batched_per_s"] = 100000 / (bst.kernel_ms / 1e3)
+        # the library's default launch shape (the S_16 bucket's tuned shape,
+        # set for the engine leg, is 2.5x slower on this easy mix); the first
+        # call on fresh slots also sizes its buffers and tables: untimed; then
+        # the median of three
+        from td16_b200 import autotune
+        out["batched_launch_shape"] = autotune.apply("defaults")
+        td.search_batch(0, inst_s[:100000], 0)
+        ms = sorted(td.search_batch(0, inst_s[:100000], 0)[1].kernel_ms for _ in range(3))
+        out["batched_per_s"] = 100000 / (ms[1] / 1e3)
     finally:
         td.destroy()
     return out

@@ -222,7 +222,9 @@ int td_search_pairs(int slot, int count, const uint8_t *beta, const uint8_t *ome
  * Results: found witnesses go to cert_writer (a td_cert_writer_open handle, or
  * NULL), and done (or NULL) receives every searched batch on a worker thread:
  * the tags given to accept, and per pair the status, depth and position
- * triples td_search_pairs returns.  Batches complete in any order. */
+ * triples td_search_pairs returns.  Batches complete in any order.  Producer
+ * threads spread over 16 filling batches with a lock each, so a batch holds
+ * pairs of the threads sharing its shard, in their order of arrival. */
 typedef void (*td_batcher_done_fn)(void *user, int count, const uint64_t *tags,
                                    const int32_t *status, const int32_t *depth,
                                    const int16_t *out_ijk);
@@ -250,9 +252,10 @@ int td_batcher_accept(void *handle, uint64_t tag, const uint8_t *beta,
                       const uint8_t *omega, int n, int initial_even_cycles,
                       float min_rate, int max_moves, int full_sorting);
 int td_batcher_flush(void *handle);
-/* Hands over the filling batch, waits for every batch to be searched and
- * delivered, and frees the consumer.  Returns TD_OK, or the first error of a
- * whole batch call (its message in err). */
+/* Hands over the filling batches, waits for every batch to be searched and
+ * delivered, and frees the consumer.  Call it once every td_batcher_accept
+ * has returned (the producers have stopped).  Returns TD_OK, or the first
+ * error of a whole batch call (its message in err). */
 int td_batcher_close(void *handle, td_batcher_stats *stats, char *err,
                      size_t errlen);
 

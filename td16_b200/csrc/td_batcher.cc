@@ -9,8 +9,10 @@
 // threads draining a bounded queue of slots + tdp.gpuQueueCapacity jobs).
 // This consumer keeps the queue model but moves batches instead of pairs:
 //
-//   accept      copies the pair into the filling batch (one mutex, no
-//               allocation in the common case) and returns; it blocks while
+//   accept      copies the pair into its thread's filling batch (16 of
+//               them, each under its own lock, so that many producer threads
+//               do not queue on one mutex; no allocation in the common case)
+//               and returns; it blocks while
 //               max_pending full batches wait for a worker, like the
 //               reference's bounded queue;
 //   delay       an idle worker takes the filling batch once its oldest pair
@@ -25,6 +27,7 @@
 //               whole batch to a completion callback.
 //
 // Only the public C ABI is used; a batch's search runs on its worker's slot.
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -75,6 +78,21 @@ struct PairBatch {
     }
 };
 
+// Producer threads spread over this many filling batches, each under its own
+// lock, so that many producers do not queue on one mutex.
+constexpr int kShards = 16;
+
+struct alignas(64) Shard {
+    std::mutex mu;
+    std::unique_ptr<PairBatch> filling;
+    std::chrono::steady_clock::time_point opened_at;
+    uint64_t pairs = 0;
+};
+
+// a producer thread's shard, assigned round-robin at its first accept
+std::atomic<unsigned> g_next_shard{0};
+thread_local int tl_shard = -1;
+
 struct Batcher {
     // configuration
     std::vector<int> slots;
@@ -87,42 +105,67 @@ struct Batcher {
     td_batcher_done_fn done = nullptr;
     void *user = nullptr;
 
-    // queue state, under mu
+    // Locks: `mu` (the ready queue) may be held while taking a shard's lock,
+    // never the other way round; `spare_mu` is taken alone.
     std::mutex mu;
     std::condition_variable cv_ready;  // idle workers: a batch is ready or started filling, or closing
     std::condition_variable cv_space;  // producers: a ready batch was taken
-    std::unique_ptr<PairBatch> filling;
-    std::chrono::steady_clock::time_point opened_at;
     std::deque<std::unique_ptr<PairBatch>> ready;
-    std::vector<std::unique_ptr<PairBatch>> spare;  // recycled buffers
+    std::atomic<size_t> ready_count{0};  // ready.size(), read without the lock by producers
     bool closed = false;
+    std::atomic<bool> closing{false};
     int idle = 0;  // workers waiting for a batch
+    Shard shards[kShards];
+    std::mutex spare_mu;
+    std::vector<std::unique_ptr<PairBatch>> spare;  // recycled buffers
 
     // statistics
-    std::atomic<uint64_t> pairs{0}, batches{0}, found{0}, not_found{0}, errors{0}, certificates{0};
+    std::atomic<uint64_t> batches{0}, found{0}, not_found{0}, errors{0}, certificates{0};
     std::atomic<uint64_t> search_ns{0};
     std::atomic<int> first_error{TD_OK};
     char first_message[256] = {0};
 
     std::vector<std::thread> workers;
 
-    std::unique_ptr<PairBatch> fresh() {  // under mu
-        if (!spare.empty()) {
-            auto b = std::move(spare.back());
-            spare.pop_back();
-            return b;
+    std::unique_ptr<PairBatch> fresh() {
+        {
+            std::lock_guard<std::mutex> g(spare_mu);
+            if (!spare.empty()) {
+                auto b = std::move(spare.back());
+                spare.pop_back();
+                return b;
+            }
         }
         auto b = std::make_unique<PairBatch>();
         b->reserve(batch_size);
         return b;
     }
 
-    // hands the filling batch to the workers (under mu)
-    void seal() {
-        if (!filling || filling->size() == 0) return;
-        ready.push_back(std::move(filling));
-        filling.reset();
+    // queues a batch for the workers (under mu)
+    void push_ready(std::unique_ptr<PairBatch> b) {
+        ready.push_back(std::move(b));
+        ready_count.store(ready.size(), std::memory_order_relaxed);
         cv_ready.notify_one();
+    }
+
+    // Moves the shards' filling batches that are due (all non-empty ones when
+    // `all`) to the ready queue; returns the earliest due time of those left.
+    // Under mu.
+    std::chrono::steady_clock::time_point sweep(bool all) {
+        const auto now = std::chrono::steady_clock::now();
+        auto earliest = std::chrono::steady_clock::time_point::max();
+        for (Shard &sh : shards) {
+            std::unique_ptr<PairBatch> b;
+            {
+                std::lock_guard<std::mutex> g(sh.mu);
+                if (!sh.filling || sh.filling->size() == 0) continue;
+                const auto due = sh.opened_at + max_delay;
+                if (all || now >= due) b = std::move(sh.filling);
+                else earliest = std::min(earliest, due);
+            }
+            if (b) push_ready(std::move(b));
+        }
+        return earliest;
     }
 
     void record_error(int rc, const char *msg) {
@@ -133,29 +176,32 @@ struct Batcher {
         }
     }
 
-    // Waits (under lk) until a batch is ready for this worker: a full one, the
+    // Waits (under lk) until a batch is ready for this worker: a full one, a
     // filling one once it is due, or what is left at close.  Returns null
     // when the consumer is closed and drained.
     std::unique_ptr<PairBatch> next_batch(std::unique_lock<std::mutex> &lk) {
         ++idle;
         for (;;) {
-            if (ready.empty() && filling && filling->size() > 0 &&
-                (closed || std::chrono::steady_clock::now() >= opened_at + max_delay))
-                seal();
-            if (!ready.empty()) break;
-            if (closed) {
-                --idle;
-                return nullptr;
+            if (ready.empty()) {
+                const auto earliest = sweep(closed);
+                if (ready.empty()) {
+                    if (closed) {
+                        --idle;
+                        return nullptr;
+                    }
+                    if (earliest != std::chrono::steady_clock::time_point::max()) cv_ready.wait_until(lk, earliest);
+                    else cv_ready.wait(lk);
+                    continue;
+                }
             }
-            if (filling && filling->size() > 0) cv_ready.wait_until(lk, opened_at + max_delay);
-            else cv_ready.wait(lk);
+            break;
         }
         --idle;
         auto b = std::move(ready.front());
         ready.pop_front();
+        ready_count.store(ready.size(), std::memory_order_relaxed);
         cv_space.notify_all();
-        // another idle worker takes over the filling batch's delay
-        if (idle > 0 && filling && filling->size() > 0) cv_ready.notify_one();
+        if (idle > 0) cv_ready.notify_one();  // another idle worker takes over the delays
         return b;
     }
 
@@ -218,7 +264,7 @@ struct Batcher {
             if (done) done(user, c, b->tag.data(), status.data(), depth.data(), ijk.data());
             batches += 1;
             b->clear();
-            std::lock_guard<std::mutex> g(mu);
+            std::lock_guard<std::mutex> g(spare_mu);
             spare.push_back(std::move(b));
         }
     }
@@ -262,30 +308,49 @@ TD_API int td_batcher_accept(void *handle, uint64_t tag, const uint8_t *beta, co
                              int initial_even_cycles, float min_rate, int max_moves, int full_sorting) {
     auto *b = static_cast<Batcher *>(handle);
     if (!b || n < 0 || n > kStride || (n > 0 && (!beta || !omega))) return TD_INVALID_ARG;
-    std::unique_lock<std::mutex> lk(b->mu);
-    while (b->ready.size() >= b->max_pending && !b->closed) b->cv_space.wait(lk);
-    if (b->closed) return TD_INVALID_ARG;
-    if (!b->filling) {
-        b->filling = b->fresh();
-        b->opened_at = std::chrono::steady_clock::now();
-        if (b->idle > 0) b->cv_ready.notify_one();  // an idle worker starts the delay
+    if (b->ready_count.load(std::memory_order_relaxed) >= b->max_pending ||
+        b->closing.load(std::memory_order_relaxed)) {
+        // the bounded queue: wait for a worker to take a batch
+        std::unique_lock<std::mutex> lk(b->mu);
+        while (b->ready.size() >= b->max_pending && !b->closed) b->cv_space.wait(lk);
+        if (b->closed) return TD_INVALID_ARG;
     }
-    PairBatch &p = *b->filling;
-    p.tag.push_back(tag);
-    const size_t at = p.beta.size();
-    p.beta.resize(at + kStride, 0);
-    p.omega.resize(at + kStride, 0);
-    if (n > 0) {
-        std::memcpy(&p.beta[at], beta, (size_t)n);
-        std::memcpy(&p.omega[at], omega, (size_t)n);
+    if (tl_shard < 0) tl_shard = (int)(g_next_shard.fetch_add(1) % kShards);
+    Shard &sh = b->shards[tl_shard];
+    std::unique_ptr<PairBatch> full;
+    bool started = false;
+    {
+        std::lock_guard<std::mutex> g(sh.mu);
+        if (!sh.filling) {
+            sh.filling = b->fresh();
+            sh.opened_at = std::chrono::steady_clock::now();
+            started = true;
+        }
+        PairBatch &p = *sh.filling;
+        p.tag.push_back(tag);
+        const size_t at = p.beta.size();
+        p.beta.resize(at + kStride, 0);
+        p.omega.resize(at + kStride, 0);
+        if (n > 0) {
+            std::memcpy(&p.beta[at], beta, (size_t)n);
+            std::memcpy(&p.omega[at], omega, (size_t)n);
+        }
+        p.n.push_back((uint8_t)n);
+        p.init.push_back(initial_even_cycles);
+        p.rate.push_back(min_rate);
+        p.max_moves.push_back(max_moves);
+        p.full.push_back(full_sorting ? 1 : 0);
+        ++sh.pairs;
+        if (p.size() >= b->batch_size) full = std::move(sh.filling);
     }
-    p.n.push_back((uint8_t)n);
-    p.init.push_back(initial_even_cycles);
-    p.rate.push_back(min_rate);
-    p.max_moves.push_back(max_moves);
-    p.full.push_back(full_sorting ? 1 : 0);
-    b->pairs += 1;
-    if (p.size() >= b->batch_size) b->seal();
+    if (full) {
+        std::lock_guard<std::mutex> g(b->mu);
+        b->push_ready(std::move(full));
+    } else if (started) {
+        // an idle worker starts this batch's delay
+        std::lock_guard<std::mutex> g(b->mu);
+        if (b->idle > 0) b->cv_ready.notify_one();
+    }
     return TD_OK;
 }
 
@@ -293,7 +358,7 @@ TD_API int td_batcher_flush(void *handle) {
     auto *b = static_cast<Batcher *>(handle);
     if (!b) return TD_INVALID_ARG;
     std::lock_guard<std::mutex> g(b->mu);
-    b->seal();
+    b->sweep(true);
     return TD_OK;
 }
 
@@ -303,9 +368,10 @@ TD_API int td_batcher_close(void *handle, td_batcher_stats *stats, char *err, si
         set_err(err, errlen, "td_batcher_close: handle is null");
         return TD_INVALID_ARG;
     }
+    b->closing.store(true);
     {
         std::lock_guard<std::mutex> g(b->mu);
-        b->seal();
+        b->sweep(true);
         b->closed = true;
     }
     b->cv_ready.notify_all();
@@ -313,7 +379,8 @@ TD_API int td_batcher_close(void *handle, td_batcher_stats *stats, char *err, si
     for (auto &t : b->workers) t.join();
     const int rc = b->first_error.load();
     if (stats) {
-        stats->pairs = b->pairs;
+        stats->pairs = 0;
+        for (Shard &sh : b->shards) stats->pairs += sh.pairs;
         stats->batches = b->batches;
         stats->found = b->found;
         stats->not_found = b->not_found;
