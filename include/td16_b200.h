@@ -152,6 +152,14 @@ int td_configure_table(int bits);
  * base >= 16 (default 16), or 0 for no restarts.  Verdicts do not depend on
  * it. */
 int td_configure_restart(int base);
+/* Reference-order batches (TD_FLAG_ORDERED, no expansion budget) run every
+ * walk on one warp for first_pass_expansions (default 64), then split each
+ * walk left over into the subtrees of its root's children, searched at once
+ * and joined in the walk's order: witness and expansion count are the
+ * one-warp walk's.  records (default 2^20, at most 2^24; 34 bytes each per
+ * slot) bounds the subtrees of one launch; a root whose children find no
+ * room runs whole.  first_pass_expansions = 0: no split. */
+int td_configure_split(int first_pass_expansions, int records);
 
 /* ---- instance preparation (host, no GPU needed) -------------------------- */
 

@@ -76,7 +76,7 @@ EXPORTS = ["td_init_slots", "td_search", "td_search_ordered", "td_slot_count", "
            "td_replay_symbols_device", "td_cert_writer_open", "td_cert_writer_enqueue", "td_cert_writer_close",
            "td_serve_open", "td_serve_workers", "td_serve_submit", "td_serve_poll", "td_serve_close",
            "td_serve_open_loop", "td_configure_percall", "td_search_pairs", "td_percall_open_loop", "td_cert_writer_enqueue_batch", "td_cert_read_file", "td_pairs_from_perms", "td_batch_graph_create", "td_batch_graph_launch", "td_batch_graph_destroy",
-           "td_batcher_open", "td_batcher_accept", "td_batcher_flush", "td_batcher_close"]
+           "td_batcher_open", "td_batcher_accept", "td_batcher_flush", "td_batcher_close", "td_configure_split"]
 
 
 def lib():
@@ -111,6 +111,7 @@ def lib():
     L.td_configure_serve.argtypes = [C.c_int, C.c_int, C.c_int]
     L.td_configure_table.argtypes = [C.c_int]
     L.td_configure_restart.argtypes = [C.c_int]
+    L.td_configure_split.argtypes = [C.c_int, C.c_int]
     L.td_set_time_limit.argtypes = [C.c_double]
     L.td_configure_percall.argtypes = [C.c_int, C.c_double, C.c_double]
     L.td_percall_open_loop.argtypes = [C.c_int, vp, C.c_int, C.c_double, C.c_uint64, C.c_int, vp,
@@ -323,6 +324,14 @@ def configure_restart(base: int) -> None:
     """Restart budgets of free-order batch searches: base x Luby sequence, 0 = none."""
     if lib().td_configure_restart(int(base)) != OK:
         raise TdError(INVALID_ARG, "restart base must be 0 or >= 16")
+
+
+def configure_split(first_pass_expansions: int = 64, records: int = 1 << 20) -> None:
+    """Reference-order batches: one-warp first pass of `first_pass_expansions`
+    (0 = no split), then walks left over split below the root into at most
+    `records` subtrees per launch.  Results do not depend on either."""
+    if lib().td_configure_split(int(first_pass_expansions), int(records)) != OK:
+        raise TdError(INVALID_ARG, "split settings: expansions >= 0, 1 <= records <= 2^24")
 
 
 def configure_percall(mode: int, rotate_after_s: float = 0.0, idle_exit_s: float = 0.0) -> None:

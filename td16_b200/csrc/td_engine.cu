@@ -82,6 +82,8 @@ __device__ __forceinline__ td_search_limits td_make_limits(uint64_t max_exp, uin
     lim.tt_gen = nullptr;
     lim.tt_bits = 0;
     lim.restart_base = 0;
+    lim.cutoff = nullptr;
+    lim.rank = 0;
     return lim;
 }
 
@@ -103,11 +105,14 @@ __global__ void __launch_bounds__(256) td_plain_kernel(const td_instance *__rest
     td_warp_search<ORDERED>(x, &out[idx], ws[warp], lut, code, codeN, lim);
 }
 
+// hard_count / hard_list (or null): instances that end with TD_ERR_BUDGET are
+// listed there, for the split pass of the reference order (td_split_*).
 template <bool ORDERED>
 __global__ void __launch_bounds__(256) td_persistent_kernel(const td_instance *__restrict__ in,
                                                            td_result *__restrict__ out, int count,
                                                            int *ticket, int grain, uint64_t max_exp,
-                                                           uint64_t time_limit_ns) {
+                                                           uint64_t time_limit_ns, int *hard_count = nullptr,
+                                                           int *hard_list = nullptr) {
     extern __shared__ __align__(16) uint8_t td_smem[];
     const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint8_t *lut = td_smem;
@@ -124,8 +129,204 @@ __global__ void __launch_bounds__(256) td_persistent_kernel(const td_instance *_
         const int last = min(count, first + grain);
         for (int idx = first; idx < last; ++idx) {
             const td_instance x = in[idx];
-            td_warp_search<ORDERED>(x, &out[idx], ws[warp], lut, code, codeN, lim);
+            const int st = td_warp_search<ORDERED>(x, &out[idx], ws[warp], lut, code, codeN, lim);
+            if (hard_list && st == TD_ERR_BUDGET && lane == 0) hard_list[atomicAdd(hard_count, 1)] = idx;
         }
+    }
+}
+
+// ---- the reference order, split below the root ------------------------------
+//
+// The reference's single-queue order is one depth-first walk, so a search
+// that runs long is a long serial chain on one warp while the rest of the GPU
+// idles: the tail of an ordered batch.  The walk visits the root's children
+// c_0, c_1, ... in a fixed order and exhausts each subtree before the next, so
+// its witness is the one it meets in the first subtree that holds any, and it
+// meets it there exactly as that subtree's own walk does.  The subtrees can
+// therefore be searched at once, one warp each, and joined in rank order: the
+// witness is the found one of lowest rank r, and the walk's expansion count
+// is 1 (the root) plus the expansions of subtrees 0..r, the earlier ones run
+// to exhaustion.  Both equal the one-warp walk's, bit for bit.  A subtree
+// that ranks after a found one stops early; its result is never read.
+//
+// Only instances that a first one-warp pass did not finish within
+// TD_SPLIT_BUDGET expansions take this path (td_persistent_kernel lists
+// them); the rest keep the first pass's results.  Passes: td_split_roots_kernel
+// lists each such root's children in visiting order, td_split_kernel searches
+// the subtrees rank-major (the first subtree of every instance, then the
+// second, ...), td_split_join_kernel writes the joined results.
+
+#define TD_SPLIT_BUDGET 64        // default expansions of the one-warp first pass (td_configure_split)
+#define TD_SPLIT_RECORDS (1 << 20)  // default subtree records per launch (32 MiB)
+#define TD_SPLIT_SKIPPED 2        // a subtree result that is never read
+
+struct td_split_ctl {
+    int hard;                   // instances the first pass did not finish
+    int max_rank;               // most children of a split root
+    int items_used;             // subtree records reserved
+    unsigned long long ticket;  // units of td_split_kernel claimed
+};
+
+// Per listed instance h (grid-stride over warps): its root's children in the
+// walk's visiting order, as position triples with bit 15 set for a child
+// accepted on visit, at kids[base[h] ..], nkids[h] of them; nkids[h] = -1
+// when the record space is full (that instance then runs whole).  Also
+// clears the instance's cutoff.
+__global__ void __launch_bounds__(256) td_split_roots_kernel(const td_instance *__restrict__ in,
+                                                            const int *__restrict__ hard_list, td_split_ctl *ctl,
+                                                            uint16_t *__restrict__ kids, int *__restrict__ base,
+                                                            int *__restrict__ nkids, int *__restrict__ cutoff,
+                                                            int records) {
+    extern __shared__ __align__(16) uint8_t td_smem[];
+    const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint8_t *lut = td_smem;
+    td_warp_smem *ws = reinterpret_cast<td_warp_smem *>(td_smem + TD_LUT_BYTES);
+    td_block_init(lut, ws, warps);
+    td_warp_smem &s = ws[warp];
+    const int H = *(volatile int *)&ctl->hard;
+    uint32_t code[TD_MAX_STEPS];
+    int codeN = -1;
+    for (int h = blockIdx.x * warps + warp; h < H; h += gridDim.x * warps) {
+        const td_instance x = in[hard_list[h]];
+        td_setup_root<true>(s, x, code, codeN);
+        const int N = x.n_symbols, T = td_triple_count(N), tb = td_tri_base(N);
+        // count the children, reserve their records, then list them (the
+        // walk consumes the root's outcome words, so the root is evaluated twice)
+        int c = 0, at = -1;
+        for (int pass = 0; pass < 2; ++pass) {
+            if (pass == 1 && at < 0) break;
+            const int odd = td_prepare_node(s, s.L[0], s.off[0], N);
+            td_evaluate(s, lut, code, (T + 31) >> 5, 0, odd, x.max_moves);
+            int k = 0;
+            for (;;) {
+                int accepted;
+                const int u = td_next_child(s, 0, &accepted);
+                if (u < 0) break;
+                if (pass == 1 && lane == 0)
+                    kids[at + k] = (uint16_t)(td_tri_table[tb + T - 1 - u] | (accepted ? 0x8000u : 0u));
+                ++k;
+            }
+            if (pass == 0) {
+                c = k;
+                if (lane == 0) {
+                    at = atomicAdd(&ctl->items_used, c);
+                    if (at > records - c) at = -1;
+                }
+                at = __shfl_sync(TD_FULL, at, 0);
+            }
+        }
+        if (lane == 0) {
+            base[h] = at;
+            nkids[h] = at < 0 ? -1 : c;
+            cutoff[h] = 0x7fffffff;  // no witness yet
+            if (at >= 0) atomicMax(&ctl->max_rank, c);
+        }
+        __syncwarp();
+    }
+}
+
+// Resident grid over the units of the split, rank-major: unit u is rank
+// r = u / H of listed instance h = u % H, i.e. subtree r of its root, or for
+// an instance without records (nkids[h] < 0) the whole search at r = 0 (so
+// the longest units start first).
+__global__ void __launch_bounds__(256) td_split_kernel(const td_instance *__restrict__ in,
+                                                      td_result *__restrict__ out, const int *__restrict__ hard_list,
+                                                      td_split_ctl *ctl, const uint16_t *__restrict__ kids,
+                                                      const int *__restrict__ base, const int *__restrict__ nkids,
+                                                      int *cutoff, td_result *__restrict__ items,
+                                                      uint64_t time_limit_ns) {
+    extern __shared__ __align__(16) uint8_t td_smem[];
+    const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint8_t *lut = td_smem;
+    td_warp_smem *ws = reinterpret_cast<td_warp_smem *>(td_smem + TD_LUT_BYTES);
+    td_block_init(lut, ws, warps);
+    td_warp_smem &s = ws[warp];
+    const int H = *(volatile int *)&ctl->hard;
+    const int R = max(1, *(volatile int *)&ctl->max_rank);
+    const unsigned long long units = (unsigned long long)H * (unsigned long long)R;
+    td_search_limits lim = td_make_limits(0, time_limit_ns, nullptr);
+    uint32_t code[TD_MAX_STEPS];
+    int codeN = -1;
+    for (;;) {
+        unsigned long long u = 0;
+        if (lane == 0) u = atomicAdd(&ctl->ticket, 1ull);
+        u = __shfl_sync(TD_FULL, u, 0);
+        if (u >= units) break;
+        const int r = (int)(u / (unsigned long long)H), h = (int)(u % (unsigned long long)H);
+        const int nk = nkids[h];
+        if (nk < 0) {
+            if (r == 0) {
+                const int idx = hard_list[h];
+                lim.cutoff = nullptr;
+                td_warp_search<true>(in[idx], &out[idx], s, lut, code, codeN, lim);
+            }
+            continue;
+        }
+        if (r >= nk) continue;  // that root has fewer children; the join reads only nkids[h]
+        td_result *it = &items[base[h] + r];
+        if (*(volatile int *)&cutoff[h] < r) {
+            td_write_result(it, TD_SPLIT_SKIPPED, 0, 0, s.path, 0, 0, 8);
+            continue;
+        }
+        const uint32_t kid = kids[base[h] + r];
+        const uint32_t t = kid & 0x7fffu;
+        const td_instance x = in[hard_list[h]];
+        td_setup_root<true>(s, x, code, codeN);
+        const int N = x.n_symbols;
+        if (lane == 0) s.path[0] = (uint16_t)t;
+        __syncwarp();
+        if (kid & 0x8000u) {  // accepted on visit: the one-move witness
+            td_write_result(it, TD_FOUND, 1, (uint16_t)t, s.path, 0, 0, 8);
+            if (lane == 0) atomicMin(&cutoff[h], r);
+            continue;
+        }
+        uint64_t nL;
+        int noff;
+        td_apply_move(s.L[0], s.off[0], N, t & 31, (t >> 5) & 31, (t >> 10) & 31, &nL, &noff);
+        if (lane == 0) {
+            s.L[1] = nL;
+            s.off[1] = (uint8_t)noff;
+        }
+        __syncwarp();
+        lim.cutoff = &cutoff[h];
+        lim.rank = r;
+        const td_dfs_out d = td_dfs<true>(s, lut, code, N, x.max_moves, 1, lim, nullptr);
+        int status = TD_NOT_FOUND;
+        if (d.status == TD_DFS_FOUND) status = TD_FOUND;
+        else if (d.status == TD_DFS_ABORTED) status = TD_SPLIT_SKIPPED;
+        else if (d.status == TD_DFS_TIMEOUT) status = TD_ERR_TIMEOUT;
+        td_write_result(it, status, status == TD_FOUND ? d.depth : 0, d.found_move, s.path, d.expansions, 0, 8);
+        if (status == TD_FOUND && lane == 0) atomicMin(&cutoff[h], r);
+    }
+}
+
+// The joined result of each split instance, as the one-warp walk would give it.
+__global__ void td_split_join_kernel(const int *__restrict__ hard_list, const td_split_ctl *ctl,
+                                     const int *__restrict__ base, const int *__restrict__ nkids,
+                                     const td_result *__restrict__ items, td_result *__restrict__ out) {
+    const int H = *(volatile const int *)&ctl->hard;
+    for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < H; h += gridDim.x * blockDim.x) {
+        const int nk = nkids[h];
+        if (nk < 0) continue;  // searched whole
+        td_result res;
+        memset(&res, 0, sizeof res);
+        res.status = TD_NOT_FOUND;
+        uint64_t exp = 1;  // the root
+        for (int r = 0; r < nk; ++r) {
+            const td_result it = items[base[h] + r];
+            if (it.status == TD_FOUND) {
+                res = it;
+                exp += it.expansions;
+                break;
+            }
+            if (it.status != TD_NOT_FOUND) {  // a subtree before any witness timed out
+                res.status = TD_ERR_TIMEOUT;
+                break;
+            }
+            exp += it.expansions;
+        }
+        res.expansions = exp > 0xffffffffull ? 0xffffffffu : (uint32_t)exp;
+        out[hard_list[h]] = res;
     }
 }
 
@@ -488,6 +689,17 @@ struct Slot {
     td_inst_state *d_state = nullptr;
     size_t state_count = 0;
     uint32_t *d_epoch = nullptr;
+    // split pass of the reference order: the listed instances, the pass's
+    // counters, each root's children, the subtree results and the cutoffs
+    int *d_hard = nullptr;
+    size_t hard_cap = 0;
+    td_split_ctl *d_split = nullptr;
+    uint16_t *d_kids = nullptr;
+    int *d_base = nullptr;
+    int *d_nkids = nullptr;
+    int *d_cutoff = nullptr;
+    td_result *d_split_items = nullptr;
+    int split_records = 0;
     // td_batch_stats of host-buffer batches: device totals and their pinned copy
     td_counts *d_counts = nullptr;
     struct HostStats {
@@ -522,6 +734,8 @@ int g_serve_split_level = 2;
 int g_serve_check_every = 32;
 int g_tt_bits = TD_TT_BITS;  // log2 entries of the explored-state tables; 0 = no table
 uint32_t g_restart_base = TD_RESTART_BASE;  // free-order restart budget base; 0 = no restarts
+int g_split_budget = TD_SPLIT_BUDGET;       // reference order: first-pass expansions before a split; 0 = none
+int g_split_records = TD_SPLIT_RECORDS;     // reference order: subtree records per launch
 
 void set_err(char *err, size_t len, const std::string &msg) {
     if (err && len) {
@@ -572,6 +786,7 @@ int preload_kernels(char *err, size_t errlen);
 struct LaunchCfg {
     int warps, grain, steal_grain, split_level, check_every, tt_bits;
     uint32_t restart_base;
+    int split_budget, split_records;
     int serve_grain, serve_split_level, serve_check_every;
     int sms, steal_blocks_per_sm, blocks_per_sm;  // of the device, for `warps`
 };
@@ -587,6 +802,8 @@ int launch_cfg(int device, LaunchCfg *c, char *err, size_t errlen) {
     c->check_every = g_check_every;
     c->tt_bits = g_tt_bits;
     c->restart_base = g_restart_base;
+    c->split_budget = g_split_budget;
+    c->split_records = g_split_records;
     c->serve_grain = g_serve_grain;
     c->serve_split_level = g_serve_split_level;
     c->serve_check_every = g_serve_check_every;
@@ -634,6 +851,8 @@ int ensure_device(int device, char *err, size_t errlen) {
     TD_CHECK(cudaFuncSetAttribute(td_persistent_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
     TD_CHECK(cudaFuncSetAttribute(td_persistent_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
     TD_CHECK(cudaFuncSetAttribute(td_steal_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
+    TD_CHECK(cudaFuncSetAttribute(td_split_roots_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
+    TD_CHECK(cudaFuncSetAttribute(td_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
     const int rc = preload_kernels(err, errlen);
     if (rc != TD_OK) return rc;
     d.ready = true;
@@ -654,6 +873,13 @@ void release_slot(Slot &s) {
     if (s.d_tt_gen) cudaFree(s.d_tt_gen);
     if (s.d_epoch) cudaFree(s.d_epoch);
     if (s.d_state) cudaFree(s.d_state);
+    if (s.d_hard) cudaFree(s.d_hard);
+    if (s.d_split) cudaFree(s.d_split);
+    if (s.d_kids) cudaFree(s.d_kids);
+    if (s.d_base) cudaFree(s.d_base);
+    if (s.d_nkids) cudaFree(s.d_nkids);
+    if (s.d_cutoff) cudaFree(s.d_cutoff);
+    if (s.d_split_items) cudaFree(s.d_split_items);
     if (s.d_counts) cudaFree(s.d_counts);
     if (s.h_stats) cudaFreeHost(s.h_stats);
     if (s.h_inst) cudaFreeHost(s.h_inst);
@@ -752,7 +978,43 @@ int launch_batch(Slot &s, int count, const td_instance *d_in, td_result *d_out, 
         const int grid_max = cfg.sms * cfg.blocks_per_sm;
         const int grid = std::max(1, std::min(grid_max, (count + warps - 1) / warps));
         TD_CHECK(cudaMemsetAsync(s.d_ticket, 0, sizeof(int), stream));
-        if (ordered)
+        if (ordered && max_exp == 0 && cfg.split_budget > 0) {
+            // one warp per instance within split_budget expansions, then the
+            // split pass for the instances left (stream-ordered buffers)
+            if (s.d_split == nullptr) TD_CHECK(cudaMallocAsync(&s.d_split, sizeof(td_split_ctl), stream));
+            if (cfg.split_records > s.split_records) {
+                if (s.d_kids) TD_CHECK(cudaFreeAsync(s.d_kids, stream));
+                if (s.d_split_items) TD_CHECK(cudaFreeAsync(s.d_split_items, stream));
+                s.d_kids = nullptr;
+                s.d_split_items = nullptr;
+                s.split_records = 0;
+                TD_CHECK(cudaMallocAsync(&s.d_kids, sizeof(uint16_t) * (size_t)cfg.split_records, stream));
+                TD_CHECK(cudaMallocAsync(&s.d_split_items, sizeof(td_result) * (size_t)cfg.split_records, stream));
+                s.split_records = cfg.split_records;
+            }
+            if ((size_t)count > s.hard_cap) {
+                for (int *p : {s.d_hard, s.d_base, s.d_nkids, s.d_cutoff})
+                    if (p) TD_CHECK(cudaFreeAsync(p, stream));
+                s.d_hard = s.d_base = s.d_nkids = s.d_cutoff = nullptr;
+                s.hard_cap = 0;
+                TD_CHECK(cudaMallocAsync(&s.d_hard, sizeof(int) * (size_t)count, stream));
+                TD_CHECK(cudaMallocAsync(&s.d_base, sizeof(int) * (size_t)count, stream));
+                TD_CHECK(cudaMallocAsync(&s.d_nkids, sizeof(int) * (size_t)count, stream));
+                TD_CHECK(cudaMallocAsync(&s.d_cutoff, sizeof(int) * (size_t)count, stream));
+                s.hard_cap = (size_t)count;
+            }
+            TD_CHECK(cudaMemsetAsync(s.d_split, 0, sizeof(td_split_ctl), stream));
+            td_persistent_kernel<true><<<grid, threads, smem, stream>>>(d_in, d_out, count, s.d_ticket, cfg.grain,
+                                                                        (uint64_t)cfg.split_budget, time_limit_ns(),
+                                                                        &s.d_split->hard, s.d_hard);
+            td_split_roots_kernel<<<grid_max, threads, smem, stream>>>(d_in, s.d_hard, s.d_split, s.d_kids, s.d_base,
+                                                                       s.d_nkids, s.d_cutoff, cfg.split_records);
+            td_split_kernel<<<grid_max, threads, smem, stream>>>(d_in, d_out, s.d_hard, s.d_split, s.d_kids, s.d_base,
+                                                                 s.d_nkids, s.d_cutoff, s.d_split_items,
+                                                                 time_limit_ns());
+            td_split_join_kernel<<<std::max(1, std::min((count + 255) / 256, 2 * cfg.sms)), 256, 0, stream>>>(
+                s.d_hard, s.d_split, s.d_base, s.d_nkids, s.d_split_items, d_out);
+        } else if (ordered)
             td_persistent_kernel<true><<<grid, threads, smem, stream>>>(d_in, d_out, count, s.d_ticket, cfg.grain,
                                                                         max_exp, time_limit_ns());
         else
@@ -1055,6 +1317,18 @@ TD_API int td_configure_table(int bits) {
 // base x luby(a) expansions in attempt a starts again with another child order
 // (td_attempt_budget, td_order_variant); 0 turns restarts off.  Verdicts do
 // not depend on it.
+// The split pass of reference-order batches: expansions of the one-warp first
+// pass (0: no split, every walk on one warp) and subtree records per launch
+// (a root whose children find no room runs whole).  Results do not depend on
+// either.
+TD_API int td_configure_split(int first_pass_expansions, int records) {
+    if (first_pass_expansions < 0 || records < 1 || records > (1 << 24)) return TD_INVALID_ARG;
+    std::lock_guard<std::mutex> g(g_mu);
+    g_split_budget = first_pass_expansions;
+    g_split_records = records;
+    return TD_OK;
+}
+
 TD_API int td_configure_restart(int base) {
     if (base < 0 || (base > 0 && base < 16)) return TD_INVALID_ARG;
     std::lock_guard<std::mutex> g(g_mu);
@@ -1677,6 +1951,9 @@ int preload_kernels(char *err, size_t errlen) {
     TD_CHECK(cudaFuncGetAttributes(&a, td_persistent_kernel<true>));
     TD_CHECK(cudaFuncGetAttributes(&a, td_persistent_kernel<false>));
     TD_CHECK(cudaFuncGetAttributes(&a, td_steal_kernel));
+    TD_CHECK(cudaFuncGetAttributes(&a, td_split_roots_kernel));
+    TD_CHECK(cudaFuncGetAttributes(&a, td_split_kernel));
+    TD_CHECK(cudaFuncGetAttributes(&a, td_split_join_kernel));
     TD_CHECK(cudaFuncGetAttributes(&a, td_epoch_kernel));
     TD_CHECK(cudaFuncGetAttributes(&a, td_finalize_kernel));
     TD_CHECK(cudaFuncGetAttributes(&a, td_count_kernel));

@@ -216,6 +216,8 @@ struct td_search_limits {
     uint32_t *tt_gen;          // this warp's generation counter of that table (kept across launches)
     int tt_bits;               // log2 of its entries
     uint32_t restart_base;     // free order: base of the restart budgets (td_attempt_budget); 0 = none
+    const int *cutoff;         // a split ordered search: lowest rank with a witness so far; null = none
+    int rank;                  // that search's own rank (it stops once *cutoff < rank)
 };
 
 __device__ __forceinline__ uint64_t td_globaltimer() {
@@ -898,9 +900,12 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
             if (lane == 0) {
                 if (lim.deadline_ns && td_globaltimer() > lim.deadline_ns) stop = 1;
                 if (lim.abort_flag && *(volatile const int *)lim.abort_flag) stop = 1;
+                // a subtree of a split ordered search: one of lower rank has a witness
+                if (lim.cutoff && *(volatile const int *)lim.cutoff < lim.rank) stop = 2;
             }
-            if (__shfl_sync(TD_FULL, stop, 0)) {
-                r.status = TD_DFS_TIMEOUT;
+            stop = __shfl_sync(TD_FULL, stop, 0);
+            if (stop) {
+                r.status = stop == 2 ? TD_DFS_ABORTED : TD_DFS_TIMEOUT;
                 break;
             }
         }
@@ -1022,9 +1027,10 @@ __device__ __forceinline__ void td_write_result(td_result *out, int status, int 
     if (lane >= w0 && lane < w1) reinterpret_cast<volatile uint32_t *>(out)[lane] = word;
 }
 
-// One complete search of instance x by the calling warp (no sharing).
+// One complete search of instance x by the calling warp (no sharing); returns
+// the status it wrote (uniform across the warp).
 template <bool ORDERED>
-__device__ void td_warp_search(const td_instance &x, td_result *out, td_warp_smem &s,
+__device__ int td_warp_search(const td_instance &x, td_result *out, td_warp_smem &s,
                                const uint8_t *lut, uint32_t (&code)[TD_MAX_STEPS], int &codeN,
                                const td_search_limits &lim) {
     int status = TD_NOT_FOUND, depth = 0;
@@ -1048,4 +1054,5 @@ __device__ void td_warp_search(const td_instance &x, td_result *out, td_warp_sme
     }
     __syncwarp();
     td_write_result(out, status, depth, found_move, s.path, expansions, 0, 8);
+    return status;
 }

@@ -157,6 +157,8 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
     lim.tt_gen = lim.tt ? tt_gen + blockIdx.x * warps + warp : nullptr;
     lim.tt_bits = tt_bits;
     lim.restart_base = 0;  // serving searches are not restarted
+    lim.cutoff = nullptr;
+    lim.rank = 0;
     td_donate_ctx dc;
     dc.ring = 1;
     dc.deadline_ns = deadline;

@@ -107,6 +107,43 @@ def test_ordered_general_pairs_rates_and_partial_sorting(slots, oracle):
     assert (res["expansions"] == np.where(N >= 3, ex + 1, 0)).all()
 
 
+def test_split_ordered_search_matches_the_one_warp_walk(slots, oracle):
+    """The reference order's split pass (searches that outlast the one-warp
+    budget are split into the subtrees of their root's children, searched at
+    once and joined in rank order): 8,192 n = 12 instances, half near-reverse,
+    at bounds 5 and 6 (both verdicts, over 1,000 walks split at bound 6).
+    Status, depth, witness and expansion count equal the oracle's walk and the
+    unsplit one-warp launch (a nonzero expansion budget keeps a batch
+    unsplit), record for record; also with a record space too small for most
+    roots (those walks run whole) and with the split off."""
+    td = slots
+    perms, n = td.synth_perms(7, 8192, 12, 12, 50, 1, 3)
+    beta, omega, init, N = _pairs(oracle, perms, n)
+    for d, hard in ((5, 1), (6, 1000)):
+        inst = td.prepare_pairs(beta, omega, N, init, 0.0, d, 1)
+        res, _ = td.search_batch(0, inst, ORDERED)
+        whole, _ = td.search_batch(1, inst, ORDERED, max_expansions=1 << 40)
+        st, dep, mv, ex = _oracle_batch(oracle, beta, omega, N, init, 0.0, d, 1)
+        assert (ex + 1 > 128).sum() >= hard
+        assert (st == 1).any() and (st == 0).any()
+        assert (res["status"] == st).all()
+        assert (res["depth"] == dep).all() and (res["moves"] == mv).all()
+        assert (res["expansions"] == ex + 1).all()
+        for key in ("status", "depth", "moves", "expansions"):
+            assert (whole[key] == res[key]).all(), key
+    # a record space too small for most roots: those walks run whole; and no split
+    inst = td.prepare_pairs(beta[:4096], omega[:4096], N[:4096], init[:4096], 0.0, 6, 1)
+    ref, _ = td.search_batch(0, inst, ORDERED)
+    try:
+        for budget, records in ((64, 300), (0, 1)):
+            td._lib.configure_split(budget, records)
+            got, _ = td.search_batch(0, inst, ORDERED)
+            for key in ("status", "depth", "moves", "expansions"):
+                assert (got[key] == ref[key]).all(), (budget, key)
+    finally:
+        td._lib.configure_split()
+
+
 def test_config2_mix_free_order_verdicts_and_replay(slots, oracle):
     """Sample of the batched uneven mix: n in {11,12,13}, 25% near-reverse,
     bound floor(n/2)+1.  Verdicts equal the oracle's; every witness replays."""
