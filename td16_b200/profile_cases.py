@@ -8,7 +8,10 @@ Every case runs with the benchmark's launch shape (td16_b200/tuned.json).
   steal    td_steal_kernel: the S_16 benchmark instances (seed 2, half
            near-reverse), bound 9, free order (default 2^18 instances)
   ordered  td_persistent_kernel<true>: 4096 x S_10 (seed 0), bound 6, the
-           reference's single-queue order
+           reference's single-queue order (with its split below the root)
+  split    td_split_kernel: 4096 x S_13 (seed 5, half near-reverse), bound
+           6, the reference's order; most walks outlast the one-warp first
+           pass and are split below the root
   plain    td_plain_kernel<false>: the plain one-launch-per-batch form on the
            first 8192 S_16 benchmark instances
   replay   td_replay_symbols_kernel: the certificates of 2^18 S_16 searches,
@@ -83,8 +86,11 @@ def run(case: str, count: int | None, table_bits: int | None = None) -> dict:
                 torch.cuda.synchronize()
                 out.update(validate_ms=a.elapsed_time(b), accepted=int(ok.sum().item()))
             return out
-        if case == "ordered":
-            perms, n = _lib.synth_perms(0, count or 4096, 10, 10, 0, 0, 0)
+        if case in ("ordered", "split"):
+            if case == "ordered":
+                perms, n = _lib.synth_perms(0, count or 4096, 10, 10, 0, 0, 0)
+            else:
+                perms, n = _lib.synth_perms(5, count or 4096, 13, 13, 50, 1, 3)
             inst = _lib.prepare_perms(perms, n, 6)
             ms, res, _, _ = _device_batch(inst, _lib.FLAG_ORDERED)
             return {"case": case, "instances": len(inst), "ms": ms, "found": int((res["status"] == 1).sum()),
@@ -123,7 +129,8 @@ def run(case: str, count: int | None, table_bits: int | None = None) -> dict:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["steal", "ordered", "plain", "replay", "validate", "serve", "percall"])
+    ap.add_argument("case", choices=["steal", "ordered", "split", "plain", "replay", "validate", "serve",
+                                         "percall"])
     ap.add_argument("--count", type=int, default=None)
     ap.add_argument("--table-bits", type=int, default=None,
                     help="entries of the explored-state tables (2^bits per warp; 0 = none; default 12)")
