@@ -426,46 +426,56 @@ __global__ void __launch_bounds__(256, TD_STEAL_MIN_BLOCKS) td_steal_kernel(cons
     dc.max_level = max_level;
     dc.check_every = check_every > 0 ? check_every : 1;
     dc.ring = 0;
+    dc.tickets = 1;
     dc.deadline_ns = lim.deadline_ns;
-    bool idle = false;
     unsigned backoff = 64;
+    // Claims.  A warp takes fresh instances by ticket while any are left, then
+    // one item ticket (fetch-and-add: it never fails) and waits until item
+    // `ticket` has been produced; items go to the waiting warps in ticket
+    // order.  (One compare-and-swap per claim attempt instead made thousands
+    // of idle warps fail on one counter, so the long searches at the end of a
+    // launch, split into thousands of items, were served a few hundred
+    // thousand items per second.)  `outstanding` counts the root units in
+    // progress plus the items not yet finished: it is raised before an
+    // instance ticket is taken and by a donor before its items can be
+    // claimed, and lowered when a unit ends.  With no instance ticket left
+    // and nothing outstanding no unit can start again, so a waiting warp may
+    // leave: its ticket is past every item there will be.
+    int my_ticket = -1;  // lane 0: this warp's item ticket, -1 = none
     for (;;) {
         int kind = 0, unit = -1;
         if (lane == 0) {
-            // `active` counts warps that hold a unit.  Counting claim attempts
-            // as well would let idle warps keep it above zero forever.  A warp
-            // that holds a unit but is not counted yet can only let others
-            // leave early; it finishes its unit itself, and it donates only to
-            // warps still waiting, so no work is left behind.
             if (*(volatile int *)&pool->inst_ticket < count) {
+                atomicAdd(&pool->outstanding, 1);
                 const int t = atomicAdd(&pool->inst_ticket, 1);
                 if (t < count) { kind = 1; unit = t; }
+                else atomicSub(&pool->outstanding, 1);
             }
             if (!kind) {
-                const int P = *(volatile int *)&pool->produced;
-                int C = *(volatile int *)&pool->consumed;
-                // one attempt per poll: a warp that loses the race backs off
-                // instead of retrying at once, which kept hundreds of idle
-                // warps hammering the one counter (n = 11..13 mix: 33 -> 25 ms)
-                if (C < P && atomicCAS(&pool->consumed, C, C + 1) == C) { kind = 2; unit = C; }
+                if (my_ticket < 0) my_ticket = atomicAdd(&pool->consumed, 1);
+                if (my_ticket < *(volatile int *)&pool->produced) {
+                    kind = 2;
+                    unit = my_ticket;
+                    my_ticket = -1;
+                }
             }
-            if (kind) atomicAdd(&pool->active, 1);
         }
         kind = __shfl_sync(TD_FULL, kind, 0);
         unit = __shfl_sync(TD_FULL, unit, 0);
         if (!kind) {
             int done = 0;
+            unsigned cap = max_backoff_ns;
             if (lane == 0) {
+                // the instance tickets first: once they are gone, an
+                // outstanding count of zero stays zero
                 const int tk = *(volatile int *)&pool->inst_ticket;
-                const int ac = *(volatile int *)&pool->active;
-                const int pr = *(volatile int *)&pool->produced;
-                const int co = *(volatile int *)&pool->consumed;
-                done = tk >= count && ac == 0 && co >= pr;
-                if (!done && !idle) { atomicAdd(&pool->idle, 1); idle = true; }
+                done = tk >= count && *(volatile int *)&pool->outstanding == 0;
                 if (!done && lim.deadline_ns && td_globaltimer() > lim.deadline_ns) {
                     atomicCAS(&pool->error, 0, TD_ERR_TIMEOUT);
                     done = 1;
                 }
+                // the next few tickets in line are served first: they poll often
+                if (my_ticket >= 0 && my_ticket - *(volatile int *)&pool->produced < 64) cap = min(cap, 512u);
             }
             if (__shfl_sync(TD_FULL, done, 0)) break;
             // waiting warps back off (to 32 us in a batch) so that their
@@ -473,11 +483,11 @@ __global__ void __launch_bounds__(256, TD_STEAL_MIN_BLOCKS) td_steal_kernel(cons
             // atomics go to; a single search (one per call) caps it lower,
             // since there the launch ends only when every waiting warp has
             // woken up and seen that the work is done
-            __nanosleep(backoff);
-            backoff = min(backoff * 2u, max_backoff_ns);
+            cap = __shfl_sync(TD_FULL, cap, 0);
+            __nanosleep(min(backoff, cap));
+            backoff = min(backoff * 2u, cap);
             continue;
         }
-        if (lane == 0 && idle) { atomicSub(&pool->idle, 1); idle = false; }
         backoff = 64;
         if (kind == 1) {
             const td_instance x = in[unit];
@@ -545,9 +555,8 @@ __global__ void __launch_bounds__(256, TD_STEAL_MIN_BLOCKS) td_steal_kernel(cons
                 td_finish_unit<false>(r, st, &out[idx], s.path);
             }
         }
-        if (lane == 0) atomicSub(&pool->active, 1);
+        if (lane == 0) atomicSub(&pool->outstanding, 1);
     }
-    if (lane == 0 && idle) atomicSub(&pool->idle, 1);
 }
 
 // Advances the launch epoch that tags donated items as written; a launch

@@ -559,10 +559,11 @@ struct td_inst_state {
 struct td_pool {
     int inst_ticket;        // next fresh instance
     int produced;           // items reserved by donors
-    int consumed;           // items claimed by takers
-    int active;             // warps inside a unit or claiming one
-    int idle;               // warps waiting for donated work
+    int consumed;           // items claimed by takers (the batch engine: item tickets taken)
+    int active;             // warps inside a unit or claiming one (the serving loop)
+    int idle;               // warps waiting for donated work (the serving loop)
     int error;              // launch-level error (bounded wait expired)
+    int outstanding;        // the batch engine: units in progress plus items not yet finished
     unsigned long long donations;
     unsigned long long donated_items;
 };
@@ -575,6 +576,7 @@ __device__ __forceinline__ uint32_t td_ring_tag(long long i) { return (uint32_t)
 
 struct td_donate_ctx {
     int ring;
+    int tickets;            // takers hold item tickets (the batch engine), see td_steal_kernel
     uint64_t deadline_ns;   // bounds the wait for a ring slot to be freed
     td_pool *pool;
     td_item *items;
@@ -641,8 +643,13 @@ __device__ __forceinline__ int td_donate(td_warp_smem &s, const td_donate_ctx &d
             if (prev == cur) { base = cur; break; }
             cur = prev;
         }
-        // the pending count must cover the items before any taker can finish one
-        if (base >= 0) atomicAdd(&dc.state->pending, give);
+        // the pending count must cover the items before any taker can finish
+        // one (takers wait for the ready flag, written below); with item
+        // tickets, so must the launch's outstanding count
+        if (base >= 0) {
+            atomicAdd(&dc.state->pending, give);
+            if (dc.tickets) atomicAdd(&dc.pool->outstanding, give);
+        }
         __threadfence();
     }
     base = __shfl_sync(TD_FULL, base, 0);
@@ -877,9 +884,15 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
                 if (lane == 0) {
                     // idle warps not yet served by an unclaimed item: without
                     // this, every busy warp would donate to the same few idle ones
-                    const int idle = *(volatile int *)&dc->pool->idle;
-                    const int unclaimed = *(volatile int *)&dc->pool->produced - *(volatile int *)&dc->pool->consumed;
-                    hungry = idle - unclaimed;
+                    if (dc->tickets) {
+                        // takers holding a ticket past the last item produced
+                        hungry = *(volatile int *)&dc->pool->consumed - *(volatile int *)&dc->pool->produced;
+                    } else {
+                        const int idle = *(volatile int *)&dc->pool->idle;
+                        const int unclaimed =
+                            *(volatile int *)&dc->pool->produced - *(volatile int *)&dc->pool->consumed;
+                        hungry = idle - unclaimed;
+                    }
                     stop = *(volatile int *)&dc->state->found;
                 }
                 stop = __shfl_sync(TD_FULL, stop, 0);

@@ -161,6 +161,7 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
     lim.rank = 0;
     td_donate_ctx dc;
     dc.ring = 1;
+    dc.tickets = 0;
     dc.deadline_ns = deadline;
     dc.pool = pool;
     dc.items = items;
