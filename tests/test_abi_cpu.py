@@ -120,6 +120,7 @@ def test_configuration_arguments_are_checked(td):
         assert lib.td_configure_restart(base) == INVALID
     assert lib.td_configure_restart(0) == td._lib.OK
     assert lib.td_configure_restart(200) == td._lib.OK
+    assert lib.td_configure_restart(16) == td._lib.OK  # the default
     for args in ((0, 2, 32), (1, -1, 32), (1, 9, 32), (1, 2, 0)):
         assert lib.td_configure_serve(*args) == INVALID
         assert lib.td_configure_steal(*args) == INVALID
