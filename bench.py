@@ -47,6 +47,9 @@ WORKLOAD = "full-size decision search: 2^20 S_16 perms, 50% uniform / 50% revers
 # (restarts, skipped children, donation and scheduling included) in
 # 95.96 M SM cycles: the ALU pipe busy 72.1 % of its 2 warp instructions per
 # cycle per SM, issue 66.4 % of 4; 0.901 GB read and 0.834 GB written.
+# Free-order searches race the search of their inverse permutation from this
+# restart attempt on (the library's default, td_configure_race).
+RACE_ATTEMPT = 8
 INST_PER_EXPANSION = 37.697e9 / 50.03e6
 ALU_INST_PER_EXPANSION = 20.491e9 / 50.03e6
 ALU_BUSY_MEASURED = 20.491e9 / (95.96e6 * 148 * 2)
@@ -388,6 +391,7 @@ def run_engine(args):
 
     from td16_b200 import autotune
     tuned = autotune.apply("17")
+    _lib.configure_race(RACE_ATTEMPT)
 
     def step(flags):
         _lib.search_batch_device(0, count, d_in.data_ptr(), d_out.data_ptr(), flags, 0, stream_ptr)
@@ -527,7 +531,7 @@ def run_engine(args):
                 "d2h_bytes_per_step": count * 32, "ms_per_step": e2e_s / e2e_steps * 1e3, "steps": len(e2e_ms),
                 "ms_min": min(e2e_ms) if e2e_ms else None, "ms_max": max(e2e_ms) if e2e_ms else None},
         "gpu_launches": args.steps * 4,  # per graph replay: epoch, search, finalize, replay
-        "launch_shape": tuned,
+        "launch_shape": {**tuned, "race_from_attempt": RACE_ATTEMPT},
         "roofline": roofline,
         "clocks": clock,
         "cpu_baseline": cpu,

@@ -74,6 +74,8 @@ typedef struct td_batch_stats {
     uint32_t launches;     /* reserved */
     uint64_t donations;    /* free-order engine: donation events */
     uint64_t donated_items;/* free-order engine: subtrees handed between warps */
+    uint64_t races;        /* free-order engine: searches raced against their
+                              inverse (td_configure_race) */
 } td_batch_stats;
 
 /* ---- slots: the reference's JNI boundary --------------------------------- */
@@ -152,6 +154,16 @@ int td_configure_table(int bits);
  * base >= 16 (default 16), or 0 for no restarts.  Verdicts do not depend on
  * it. */
 int td_configure_restart(int base);
+/* Free-order batch searches of full-sorting instances with restarts on and
+ * no expansion budget: a search that starts restart attempt `attempt`
+ * (1..32, the 32nd being the last, unbounded one) also queues the search of
+ * its inverse permutation, which another warp runs alongside; the first
+ * witness (turned into the instance's positions) or the first side searched
+ * to the end decides.  A permutation and its inverse are equally far from
+ * sorted, so verdicts do not depend on it.  Default 8; 0 turns the race
+ * off.  No counterpart in the reference, whose search runs one order to the
+ * end. */
+int td_configure_race(int attempt);
 /* Reference-order batches (TD_FLAG_ORDERED, no expansion budget) run every
  * walk on one warp for first_pass_expansions (default 64), then split each
  * walk left over into the subtrees of its root's children, searched at once

@@ -477,3 +477,22 @@ extern "C" int td_emu_search_batch(int count, const td_instance *x, unsigned fla
 // The engine's device replay of a witness (td_witness_ok, the rule of
 // TD_FLAG_VERIFY), for the CPU tests.
 extern "C" int td_emu_witness_ok(const td_instance *x, const td_result *r) { return td_witness_ok(*x, *r); }
+
+// The inverse instance and the conversion of its witnesses (td_core.cuh:
+// td_inverse_pinned, td_witness_from_inverse), which the batch engine's race
+// of a search against the search of its inverse uses; for the CPU tests.
+extern "C" void td_emu_inverse_instance(const td_instance *x, td_instance *out) {
+    *out = *x;
+    out->perm = td_inverse_pinned(x->perm, x->n_symbols);
+    out->offset = 0;
+}
+
+extern "C" int td_emu_witness_from_inverse(const td_instance *x, const td_result *inv, td_result *out) {
+    *out = *inv;
+    return td_witness_from_inverse(x->perm, x->offset, x->n_symbols, inv->moves, inv->depth, out->moves);
+}
+
+extern "C" int td_emu_pinned_cycles(uint64_t L, int off, int N) {
+    uint32_t fixed;
+    return td_pinned_cycles(L, off, N, &fixed);
+}

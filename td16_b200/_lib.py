@@ -28,7 +28,7 @@ assert INSTANCE_DTYPE.itemsize == 16 and RESULT_DTYPE.itemsize == 32
 class BatchStats(C.Structure):
     _fields_ = [("expansions", C.c_uint64), ("found", C.c_uint64), ("not_found", C.c_uint64),
                 ("errors", C.c_uint64), ("kernel_ms", C.c_float), ("launches", C.c_uint32),
-                ("donations", C.c_uint64), ("donated_items", C.c_uint64)]
+                ("donations", C.c_uint64), ("donated_items", C.c_uint64), ("races", C.c_uint64)]
 
 
 class ServeStats(C.Structure):
@@ -70,7 +70,7 @@ _lib = None
 EXPORTS = ["td_init_slots", "td_search", "td_search_ordered", "td_slot_count", "td_slot_device",
            "td_slot_stream", "td_destroy", "td_prepare_pairs", "td_prepare_perms", "td_synth_perms",
            "td_search_batch", "td_search_batch_device", "td_validate_batch_device",
-           "td_positions_to_symbols", "td_configure", "td_configure_steal", "td_configure_serve", "td_configure_table", "td_configure_restart",
+           "td_positions_to_symbols", "td_configure", "td_configure_steal", "td_configure_serve", "td_configure_table", "td_configure_restart", "td_configure_race",
            "td_set_time_limit", "td_int_issue_peak",
            "td_codec_key", "td_codec_value", "td_codec_decode_key", "td_codec_decode_value",
            "td_replay_symbols_device", "td_cert_writer_open", "td_cert_writer_enqueue", "td_cert_writer_close",
@@ -111,6 +111,7 @@ def lib():
     L.td_configure_serve.argtypes = [C.c_int, C.c_int, C.c_int]
     L.td_configure_table.argtypes = [C.c_int]
     L.td_configure_restart.argtypes = [C.c_int]
+    L.td_configure_race.argtypes = [C.c_int]
     L.td_configure_split.argtypes = [C.c_int, C.c_int]
     L.td_set_time_limit.argtypes = [C.c_double]
     L.td_configure_percall.argtypes = [C.c_int, C.c_double, C.c_double]
@@ -324,6 +325,14 @@ def configure_restart(base: int) -> None:
     """Restart budgets of free-order batch searches: base x Luby sequence, 0 = none."""
     if lib().td_configure_restart(int(base)) != OK:
         raise TdError(INVALID_ARG, "restart base must be 0 or >= 16")
+
+
+def configure_race(attempt: int) -> None:
+    """Free-order batches: a search that starts restart attempt `attempt`
+    (1..32) races a search of its inverse permutation; 0 = off.  Verdicts do
+    not depend on it."""
+    if lib().td_configure_race(int(attempt)) != OK:
+        raise TdError(INVALID_ARG, "race attempt: 0..32")
 
 
 def configure_split(first_pass_expansions: int = 64, records: int = 1 << 20) -> None:

@@ -421,6 +421,81 @@ TD_HD int td_witness_ok(const td_instance &x, const td_result &r) {
     return td_accepts(N, td_inst_init(x), x.min_rate, td_inst_full(x), odd, r.depth);
 }
 
+// ---- the inverse instance (free order, full sorting) ------------------------
+//
+// A permutation and its inverse are the same number of transpositions from
+// the identity, and a witness for one gives one for the other.  Searches of
+// the two often differ by orders of magnitude in expansions, so the batch
+// engine races them (td_steal_kernel).  In pinned form the inverse of the
+// state (L, off) is L^-1 (nibble L[m] holds m) with the caller's array
+// starting at pinned position 0; its odd-cycle count equals that of (L, off),
+// so the acceptance and pruning masks of full sorting carry over unchanged.
+
+TD_HD uint64_t td_inverse_pinned(uint64_t L, int N) {
+    uint64_t R = 0;
+    for (int m = 0; m < 16; ++m) R |= (uint64_t)m << (4 * (m < N - 1 ? (int)td_nib(L, m) : m));
+    return R;
+}
+
+// The caller's array of the pinned state (L, off): the label at each caller
+// position (pinned position c + off mod N holds B[p] = p ? L[p-1]+1 : 0).
+TD_HD void td_caller_array(uint64_t L, int off, int N, uint8_t *A) {
+    for (int c = 0; c < N; ++c) {
+        int p = c + off;
+        p -= p >= N ? N : 0;
+        A[c] = p ? (uint8_t)(td_nib(L, p - 1) + 1u) : (uint8_t)0;
+    }
+}
+
+// The caller-position move (i, j, k) on an array: blocks [i, j) and [j, k)
+// change places.
+TD_HD void td_swap_blocks(uint8_t *A, int i, int j, int k) {
+    uint8_t t[TD_MAX_N];
+    for (int m = i; m < k; ++m) t[m] = A[m];
+    for (int m = i; m < k; ++m) A[m] = m < i + (k - j) ? t[m + (j - i)] : t[m - (k - j)];
+}
+
+// A witness of the inverse instance (td_inverse_pinned(L, N), offset 0):
+// inv[0..k-1] in its caller positions -> the witness of (L, off) in the
+// caller's positions, out[0..k-1].  Returns 0 if the moves do not fit.
+//
+// With A the caller's array and B the inverse's, B = R_off . A^-1 (R_s: the
+// rotation c -> c + s).  If B . s_1 ... s_k is sorted (a rotation), then
+// A = (s_1 ... s_k) . R_u for some u, and the answer A . t_1 ... t_k passes,
+// up to a rotation of positions, through the arrays S_m = s_1 ... s_m (the
+// identity array after the moves s_1..s_m) for m = k, k-1, ..., 0.  The step
+// from S_m to S_{m-1} is the block swap s_m^-1 = (i, i + k - j, k).  A block
+// swap of a cyclic array is fixed by its three cut points, so t is the block
+// swap of the caller's current array at the cuts between the same two
+// neighbouring labels.
+TD_HD int td_witness_from_inverse(uint64_t L, int off, int N, const uint16_t *inv, int k, uint16_t *out) {
+    uint8_t X[TD_MAX_N], S[TD_MAX_N];
+    td_caller_array(L, off, N, X);
+    for (int m = k; m >= 1; --m) {
+        for (int p = 0; p < N; ++p) S[p] = (uint8_t)p;
+        for (int q = 0; q < m; ++q) td_swap_blocks(S, inv[q] & 31, (inv[q] >> 5) & 31, (inv[q] >> 10) & 31);
+        const int i = inv[m - 1] & 31, j = (inv[m - 1] >> 5) & 31, kk = (inv[m - 1] >> 10) & 31;
+        if (!(i < j && j < kk && kk < N)) return 0;
+        const int g[3] = {i, i + kk - j, kk};
+        int c3[3];
+        for (int t = 0; t < 3; ++t) {
+            const uint8_t u = S[g[t] == 0 ? N - 1 : g[t] - 1], v = S[g[t]];
+            c3[t] = -1;
+            for (int c = 0; c < N; ++c)
+                if (X[c == 0 ? N - 1 : c - 1] == u && X[c] == v) { c3[t] = c; break; }
+            if (c3[t] < 0) return 0;
+        }
+        // ascending order
+        if (c3[0] > c3[1]) { const int w = c3[0]; c3[0] = c3[1]; c3[1] = w; }
+        if (c3[1] > c3[2]) { const int w = c3[1]; c3[1] = c3[2]; c3[2] = w; }
+        if (c3[0] > c3[1]) { const int w = c3[0]; c3[0] = c3[1]; c3[1] = w; }
+        if (!(c3[0] < c3[1] && c3[1] < c3[2])) return 0;
+        out[k - m] = td_pack_move(c3[0], c3[1], c3[2]);
+        td_swap_blocks(X, c3[0], c3[1], c3[2]);
+    }
+    return 1;
+}
+
 // ---- instance preparation (host side) --------------------------------------
 
 // Odd-length cycles of omega, fixed points included (sorting_search.cu:211-226).

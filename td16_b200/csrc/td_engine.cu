@@ -43,6 +43,7 @@ struct td_batch_stats {
     float kernel_ms;
     uint32_t launches;
     uint64_t donations, donated_items;
+    uint64_t races;
 };
 
 static_assert(sizeof(td_instance) == 16, "td_instance layout");
@@ -338,6 +339,11 @@ __global__ void td_split_join_kernel(const int *__restrict__ hard_list, const td
 // Ends one unit of a shared search: records a found witness (first finder
 // wins), and the unit that finishes the search last writes the final status
 // and the summed expansions.  Returns 1 in the warp that finished last.
+// `side` 1 marks a unit of the inverse instance's search (td_steal_kernel's
+// race; its witness is already in the instance's positions).  When the last
+// unit of one side ends with no witness and no error recorded, that side's
+// whole tree was searched: the instance has no witness within the bound, and
+// found = 2 stops the other side.
 // HOST_OUT: `out` is host memory mapped into the device (the serving loop), so
 // the fences are system-scope; the batch engine's results are device memory,
 // where device-scope fences order the same writes at a fraction of the cost.
@@ -349,7 +355,7 @@ __device__ __forceinline__ void td_unit_fence() {
 
 template <bool HOST_OUT>
 __device__ __forceinline__ int td_finish_unit(const td_dfs_out &r, td_inst_state *st, td_result *out,
-                                              const uint16_t *path) {
+                                              const uint16_t *path, int side = 0) {
     const int lane = threadIdx.x & 31;
     int win = 0, last = 0;
     if (lane == 0) {
@@ -363,8 +369,13 @@ __device__ __forceinline__ int td_finish_unit(const td_dfs_out &r, td_inst_state
     __syncwarp();
     if (lane == 0) {
         td_unit_fence<HOST_OUT>();
-        last = atomicSub(&st->pending, 1) == 1;
+        const int unit = side ? 1 << 16 : 1;
+        const int before = atomicSub(&st->pending, unit);
+        last = before == unit;
         if (last) td_unit_fence<HOST_OUT>();
+        else if (((before - unit) & (side ? 0xffff0000 : 0x0000ffff)) == 0 &&
+                 *(volatile int *)&st->found == 0 && *(volatile int *)&st->error == 0)
+            atomicCAS(&st->found, 0, 2);
     }
     last = __shfl_sync(TD_FULL, last, 0);
     if (last) {
@@ -378,8 +389,8 @@ __device__ __forceinline__ int td_finish_unit(const td_dfs_out &r, td_inst_state
         found = __shfl_sync(TD_FULL, found, 0);
         err = __shfl_sync(TD_FULL, err, 0);
         exp = __shfl_sync(TD_FULL, exp, 0);
-        if (!found) td_write_result(out, err ? err : TD_NOT_FOUND, 0, 0, path, exp, 0, 8);
-        else td_write_result(out, TD_FOUND, 0, 0, path, exp, 7, 8);
+        if (found == 1) td_write_result(out, TD_FOUND, 0, 0, path, exp, 7, 8);
+        else td_write_result(out, found == 2 || !err ? TD_NOT_FOUND : err, 0, 0, path, exp, 0, 8);
         __syncwarp();
     }
     return last;
@@ -395,7 +406,7 @@ __global__ void __launch_bounds__(256, TD_STEAL_MIN_BLOCKS) td_steal_kernel(cons
                                                       int max_level, int check_every, uint64_t time_limit_ns,
                                                       uint64_t *tt, uint32_t *tt_gen, int tt_bits,
                                                       uint32_t restart_base, uint64_t max_exp,
-                                                      unsigned max_backoff_ns) {
+                                                      unsigned max_backoff_ns, int race, int spawn_base) {
     extern __shared__ __align__(16) uint8_t td_smem[];
     const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // free order only: no class table, the warp frames start the block's shared memory
@@ -421,7 +432,12 @@ __global__ void __launch_bounds__(256, TD_STEAL_MIN_BLOCKS) td_steal_kernel(cons
     dc.ready = ready;
     const uint32_t epoch = *epoch_ptr;  // bumped by td_epoch_kernel before this launch
     dc.epoch = epoch;
-    dc.capacity = capacity;
+    // race: donated items use slots [0, spawn_base), queued inverse roots the rest
+    dc.capacity = race ? spawn_base : capacity;
+    dc.spawn_base = spawn_base;
+    dc.spawn_capacity = race ? capacity - spawn_base : 0;
+    dc.side = 0;
+    dc.race = 0;
     dc.grain = grain;
     dc.max_level = max_level;
     dc.check_every = check_every > 0 ? check_every : 1;
@@ -441,7 +457,19 @@ __global__ void __launch_bounds__(256, TD_STEAL_MIN_BLOCKS) td_steal_kernel(cons
     // claimed, and lowered when a unit ends.  With no instance ticket left
     // and nothing outstanding no unit can start again, so a waiting warp may
     // leave: its ticket is past every item there will be.
+    //
+    // Race (`race` = a, 0: off): a root search of a full-sorting instance
+    // that starts its restart attempt a queues the instance's inverse
+    // (td_spawn_inverse).  Queued inverses are claimed once no fresh instance
+    // is left, before donated items, by their own tickets (fetch-and-add,
+    // taken only while some are queued).  While fresh instances remain every
+    // warp is busy, and a second search of an instance would only displace
+    // other work; at the end of the launch, where warps idle, it shortens the
+    // longest searches.  Most queued inverses belong to instances decided by
+    // then and end at once.  A ticket taken past the last inverse queued is
+    // kept until one is queued for it.
     int my_ticket = -1;  // lane 0: this warp's item ticket, -1 = none
+    int my_spawn = -1;   // lane 0: this warp's ticket of the queue of inverses, -1 = none
     for (;;) {
         int kind = 0, unit = -1;
         if (lane == 0) {
@@ -450,6 +478,17 @@ __global__ void __launch_bounds__(256, TD_STEAL_MIN_BLOCKS) td_steal_kernel(cons
                 const int t = atomicAdd(&pool->inst_ticket, 1);
                 if (t < count) { kind = 1; unit = t; }
                 else atomicSub(&pool->outstanding, 1);
+            }
+            if (!kind && race) {
+                // slots past the queue's capacity are never claimed
+                const int queued = min(*(volatile int *)&pool->spawn_produced, dc.spawn_capacity);
+                if (my_spawn < 0 && *(volatile int *)&pool->spawn_consumed < queued)
+                    my_spawn = atomicAdd(&pool->spawn_consumed, 1);
+                if (my_spawn >= 0 && my_spawn < min(*(volatile int *)&pool->spawn_produced, dc.spawn_capacity)) {
+                    kind = 3;
+                    unit = my_spawn;
+                    my_spawn = -1;
+                }
             }
             if (!kind) {
                 if (my_ticket < 0) my_ticket = atomicAdd(&pool->consumed, 1);
@@ -499,15 +538,20 @@ __global__ void __launch_bounds__(256, TD_STEAL_MIN_BLOCKS) td_steal_kernel(cons
                 td_setup_root<false>(s, x, code, codeN);
                 dc.inst = (uint32_t)unit;
                 dc.state = st;
+                dc.side = 0;
+                dc.race = td_inst_full(x) ? race : 0;
                 const td_dfs_out r = td_dfs<false>(s, lut, code, x.n_symbols, x.max_moves, 0, lim, &dc);
+                dc.race = 0;
                 td_finish_unit<false>(r, st, &out[unit], s.path);
             }
         } else {
-            // wait until the donor has written the item (bounded)
+            // a donated item (kind 2) or a queued inverse root (kind 3); wait
+            // until its producer has written it (bounded)
+            const int phys = kind == 3 ? spawn_base + unit : unit;
             int ok = 0;
             if (lane == 0) {
                 for (unsigned spin = 0; spin < (1u << 30); ++spin) {
-                    if (*(volatile uint32_t *)&ready[unit] == epoch) { ok = 1; break; }
+                    if (*(volatile uint32_t *)&ready[phys] == epoch) { ok = 1; break; }
                     if ((spin & 1023u) == 0 && lim.deadline_ns && td_globaltimer() > lim.deadline_ns) break;
                     __nanosleep(32);
                 }
@@ -518,16 +562,26 @@ __global__ void __launch_bounds__(256, TD_STEAL_MIN_BLOCKS) td_steal_kernel(cons
             if (ok) {
                 td_item it;  // read through L2: the donor wrote it from another SM
                 {
-                    const uint4 *src = reinterpret_cast<const uint4 *>(&items[unit]);
+                    const uint4 *src = reinterpret_cast<const uint4 *>(&items[phys]);
                     uint4 *dst = reinterpret_cast<uint4 *>(&it);
                     dst[0] = __ldcg(src);
                     dst[1] = __ldcg(src + 1);
                 }
                 const uint32_t idx = it.inst;
+                const int d0 = it.depth & 0x7f;
+                const int side = it.depth >> 7;
+                // an item names an instance of this launch and a level of the
+                // frame; one that does not is a launch error, never followed
+                if (idx >= (uint32_t)count || d0 >= TD_MAX_DEPTH || (kind == 3) != (side && d0 == 0)) {
+                    if (lane == 0) {
+                        atomicCAS(&pool->error, 0, TD_ERR_VERIFY);
+                        atomicSub(&pool->outstanding, 1);
+                    }
+                    continue;
+                }
                 const td_instance x = in[idx];
                 td_inst_state *st = &state[idx];
                 td_setup_root<false>(s, x, code, codeN);
-                const int d0 = it.depth;
                 if (lane == 0) {
                     s.L[d0] = it.L;
                     s.off[d0] = it.off;
@@ -545,14 +599,23 @@ __global__ void __launch_bounds__(256, TD_STEAL_MIN_BLOCKS) td_steal_kernel(cons
                     r.expansions = 0;
                 } else {
                     // a donated subtree is searched once, to the end: restarting it
-                    // would only repeat work when it holds no witness
+                    // would only repeat work when it holds no witness; the root of
+                    // an inverse instance restarts like any root search
                     td_search_limits ilim = lim;
-                    ilim.restart_base = 0;
+                    if (d0 > 0) ilim.restart_base = 0;
                     dc.inst = idx;
                     dc.state = st;
+                    dc.side = side;
                     r = td_dfs<false>(s, lut, code, x.n_symbols, x.max_moves, d0, ilim, &dc);
+                    dc.side = 0;
+                    // a witness of the inverse becomes one of the instance; one that
+                    // does not convert is reported as a failed replay, never recorded
+                    if (side && r.status == TD_DFS_FOUND && !td_inverse_result(s, x, r)) {
+                        r.status = TD_DFS_EXHAUSTED;
+                        if (lane == 0) atomicCAS(&st->error, 0, TD_ERR_VERIFY);
+                    }
                 }
-                td_finish_unit<false>(r, st, &out[idx], s.path);
+                td_finish_unit<false>(r, st, &out[idx], s.path, side);
             }
         }
         if (lane == 0) atomicSub(&pool->outstanding, 1);
@@ -745,6 +808,7 @@ int g_tt_bits = TD_TT_BITS;  // log2 entries of the explored-state tables; 0 = n
 uint32_t g_restart_base = TD_RESTART_BASE;  // free-order restart budget base; 0 = no restarts
 int g_split_budget = TD_SPLIT_BUDGET;       // reference order: first-pass expansions before a split; 0 = none
 int g_split_records = TD_SPLIT_RECORDS;     // reference order: subtree records per launch
+int g_race = 8;  // free-order batches: attempt at which a search starts racing its inverse, 0 = off (td_configure_race)
 
 void set_err(char *err, size_t len, const std::string &msg) {
     if (err && len) {
@@ -795,6 +859,7 @@ int preload_kernels(char *err, size_t errlen);
 struct LaunchCfg {
     int warps, grain, steal_grain, split_level, check_every, tt_bits;
     uint32_t restart_base;
+    int race;
     int split_budget, split_records;
     int serve_grain, serve_split_level, serve_check_every;
     int sms, steal_blocks_per_sm, blocks_per_sm;  // of the device, for `warps`
@@ -811,6 +876,7 @@ int launch_cfg(int device, LaunchCfg *c, char *err, size_t errlen) {
     c->check_every = g_check_every;
     c->tt_bits = g_tt_bits;
     c->restart_base = g_restart_base;
+    c->race = g_race;
     c->split_budget = g_split_budget;
     c->split_records = g_split_records;
     c->serve_grain = g_serve_grain;
@@ -976,10 +1042,16 @@ int launch_batch(Slot &s, int count, const td_instance *d_in, td_result *d_out, 
         TD_CHECK(cudaMemsetAsync(s.d_pool, 0, sizeof(td_pool), stream));
         TD_CHECK(cudaMemsetAsync(s.d_state, 0, (size_t)count * sizeof(td_inst_state), stream));
         td_epoch_kernel<<<1, 1, 0, stream>>>(s.d_epoch);
+        // the race needs restarts, and an expansion budget per unit would make
+        // one side's budget decide the other's; its queue of inverse roots
+        // holds one slot per instance (each queues its inverse at most once),
+        // at the top of the item space, which keeps at least half for donation
+        const int race = cfg.restart_base > 0 && max_exp == 0 && count <= s.item_capacity / 2 ? cfg.race : 0;
+        const int spawn_base = race ? s.item_capacity - count : s.item_capacity;
         td_steal_kernel<<<grid, threads, steal_smem_bytes(warps), stream>>>(
             d_in, d_out, count, s.d_pool, s.d_items, s.d_ready, s.d_epoch, s.item_capacity, s.d_state,
             cfg.steal_grain, cfg.split_level, cfg.check_every, time_limit_ns(), cfg.tt_bits > 0 ? s.d_tt : nullptr,
-            s.d_tt_gen, cfg.tt_bits, cfg.restart_base, max_exp, count == 1 ? 4096u : 32768u);
+            s.d_tt_gen, cfg.tt_bits, cfg.restart_base, max_exp, count == 1 ? 4096u : 32768u, race, spawn_base);
         TD_CHECK(cudaGetLastError());
         td_finalize_kernel<<<std::max(1, std::min((count + 255) / 256, 2 * cfg.sms)), 256, 0, stream>>>(
             s.d_pool, s.d_state, d_out, count);
@@ -1345,6 +1417,16 @@ TD_API int td_configure_restart(int base) {
     return TD_OK;
 }
 
+// Later free-order batches (full sorting) race a search that starts its
+// restart attempt `attempt` (1..32; the 32nd is the last, unbounded one)
+// against a search of its inverse instance; 0 turns the race off.
+TD_API int td_configure_race(int attempt) {
+    if (attempt < 0 || attempt > TD_RESTARTS) return TD_INVALID_ARG;
+    std::lock_guard<std::mutex> g(g_mu);
+    g_race = attempt;
+    return TD_OK;
+}
+
 // Work distribution of later serving launches (td_serve_open): items per
 // donation, deepest level whose children are donated, expansions between
 // idle checks.
@@ -1512,6 +1594,7 @@ TD_API int td_search_batch(int slot, int count, const td_instance *in, td_result
             const td_pool &pool = s->h_stats->pool;
             stats->donations = pool.donations;
             stats->donated_items = pool.donated_items;
+            stats->races = (uint64_t)pool.spawn_produced;
             if (pool.error) {
                 set_err(err, errlen, "engine launch deadline reached");
                 return TD_TIMEOUT;
@@ -1858,7 +1941,8 @@ TD_API int td_search_batch_noalloc(int count, const td_instance *d_instances, td
         const int grid = d.sms * std::max(1, d.steal_blocks);
         td_steal_kernel<<<grid, threads, steal_smem_bytes(warps), st>>>(
             d_instances, d_results, count, pool, items, ready, epoch, TD_NOALLOC_ITEMS, state, grain, split_level,
-            check_every, limit, nullptr, nullptr, 0, restart_base, max_exp, count == 1 ? 4096u : 32768u);
+            check_every, limit, nullptr, nullptr, 0, restart_base, max_exp, count == 1 ? 4096u : 32768u,
+            /*race=*/0, /*spawn_base=*/TD_NOALLOC_ITEMS);
         TD_CHECK_NA(cudaGetLastError());
         td_finalize_kernel<<<std::max(1, std::min((count + 255) / 256, 2 * d.sms)), 256, 0, st>>>(pool, state,
                                                                                                 d_results, count);

@@ -542,15 +542,19 @@ __device__ __forceinline__ int td_next_child_rows(td_warp_smem &s, const uint32_
 struct __align__(16) td_item {  // 32 bytes
     uint64_t L;
     uint32_t inst;          // instance index
-    uint8_t depth;          // >= 1
+    uint8_t depth;          // bits 0-6: DFS depth of the node (0 only for the root of an inverse
+                            // instance); bit 7: the node belongs to the inverse instance's search
     uint8_t off;
     uint16_t path[TD_MAX_DEPTH];
 };
 
 // Per-instance bookkeeping when several warps share one search.
 struct td_inst_state {
-    int found;              // set once by the warp that records the witness
-    int pending;            // units (the root search + items) not yet finished
+    int found;              // 1: a warp recorded the witness; 2: one side of a race was searched
+                            // to the end without one (the verdict is known, the other side stops)
+    int pending;            // units (the root search + items) not yet finished: the low 16 bits
+                            // count the search of the instance, the high 16 bits that of its
+                            // inverse (td_steal_kernel's race; elsewhere only the low half is used)
     unsigned expansions;    // summed over units
     int error;              // first error status seen (timeout)
 };
@@ -564,6 +568,8 @@ struct td_pool {
     int idle;               // warps waiting for donated work (the serving loop)
     int error;              // launch-level error (bounded wait expired)
     int outstanding;        // the batch engine: units in progress plus items not yet finished
+    int spawn_produced;     // the batch engine's race: inverse roots queued
+    int spawn_consumed;     // and claimed
     unsigned long long donations;
     unsigned long long donated_items;
 };
@@ -588,6 +594,11 @@ struct td_donate_ctx {
     int check_every;        // expansions between idle checks
     uint32_t inst;
     td_inst_state *state;
+    int side;               // 1: the unit searches the instance's inverse (items carry it on)
+    int race;               // > 0: the unit queues its inverse when it starts restart attempt
+                            // `race` (root units of full-sorting instances in td_steal_kernel)
+    int spawn_base;         // the race's queue: item slots [spawn_base, spawn_base + spawn_capacity)
+    int spawn_capacity;
 };
 
 #define TD_DFS_FOUND 1
@@ -647,7 +658,7 @@ __device__ __forceinline__ int td_donate(td_warp_smem &s, const td_donate_ctx &d
         // one (takers wait for the ready flag, written below); with item
         // tickets, so must the launch's outstanding count
         if (base >= 0) {
-            atomicAdd(&dc.state->pending, give);
+            atomicAdd(&dc.state->pending, dc.side ? give << 16 : give);
             if (dc.tickets) atomicAdd(&dc.pool->outstanding, give);
         }
         __threadfence();
@@ -678,7 +689,7 @@ __device__ __forceinline__ int td_donate(td_warp_smem &s, const td_donate_ctx &d
         td_item it;
         it.L = nL;
         it.inst = dc.inst;
-        it.depth = (uint8_t)(lv + 1);
+        it.depth = (uint8_t)((lv + 1) | (dc.side << 7));
         it.off = (uint8_t)noff;
 #pragma unroll
         for (int d = 0; d < TD_MAX_DEPTH; ++d) it.path[d] = d < lv ? s.path[d] : (d == lv ? (uint16_t)t : 0);
@@ -721,6 +732,105 @@ __device__ __forceinline__ int td_donate(td_warp_smem &s, const td_donate_ctx &d
     }
     __syncwarp();
     return give;
+}
+
+// Queues the inverse of the unit's instance (td_inverse_pinned) as a root item
+// of the race's queue, so that another warp searches it while this one goes
+// on; the first witness on either side ends both, and so does either side
+// searched to the end without one (found = 2).  The pending and outstanding
+// counts cover the item before it can be claimed.  Only an instance's root
+// search queues its inverse, once, and the queue holds a slot per instance of
+// the launch, so one fetch-and-add reserves a slot: busy searches queue their
+// inverses at up to several per microsecond, and a compare-and-swap loop on
+// the counter kept them waiting.  Returns whether it was queued (uniform
+// across the warp).
+__device__ __forceinline__ int td_spawn_inverse(const td_warp_smem &s, const td_donate_ctx &dc, int N) {
+    int ok = 0;
+    if ((threadIdx.x & 31) == 0) {
+        const int slot = atomicAdd(&dc.pool->spawn_produced, 1);
+        if (slot < dc.spawn_capacity) {
+            atomicAdd(&dc.state->pending, 1 << 16);
+            atomicAdd(&dc.pool->outstanding, 1);
+            td_item it;
+            it.L = td_inverse_pinned(s.L[0], N);
+            it.inst = dc.inst;
+            it.depth = 0x80;
+            it.off = 0;
+#pragma unroll
+            for (int d = 0; d < TD_MAX_DEPTH; ++d) it.path[d] = 0;
+            dc.items[dc.spawn_base + slot] = it;
+            __threadfence();
+            atomicExch(&dc.ready[dc.spawn_base + slot], dc.epoch);
+            ok = 1;
+        }
+    }
+    return __shfl_sync(TD_FULL, ok, 0);
+}
+
+// After a unit of the inverse's search found a witness (depth moves: path[0 ..
+// depth-2] and found_move), rewrites it as the witness of the instance x in
+// the caller's positions: td_witness_from_inverse's steps, one lane per
+// position (arrays in registers, block swaps by shuffle, cut points by
+// ballot).  Returns 0 if it does not convert (then no witness may be
+// recorded).  Uniform across the warp.
+__device__ __forceinline__ int td_inverse_result(td_warp_smem &s, const td_instance &x, td_dfs_out &r) {
+    const int c = threadIdx.x & 31;
+    const int N = x.n_symbols, k = r.depth;
+    if (k < 1 || k > TD_MAX_DEPTH) return 0;
+    // the swap of blocks [i, j) and [j, kk) moves the value at src(c) to c
+    auto swap = [&](uint32_t v, uint32_t mv) {
+        const int i = mv & 31, j = (mv >> 5) & 31, kk = (mv >> 10) & 31;
+        int src = c;
+        if (c >= i && c < kk) src = c < i + (kk - j) ? c + (j - i) : c - (kk - j);
+        return __shfl_sync(TD_FULL, v, src);
+    };
+    // lane q holds the inverse's move q; the converted moves then go to s.path
+    const uint32_t inv = c < k - 1 ? (uint32_t)s.path[c] : (c == k - 1 ? (uint32_t)r.found_move : 0u);
+    __syncwarp();
+    // X: the caller's array; S: the identity array after all the inverse's moves
+    int p = c + x.offset;
+    p -= p >= N ? N : 0;
+    uint32_t X = c < N ? (p ? td_nib(x.perm, p - 1) + 1u : 0u) : 0xffu;
+    uint32_t S = (uint32_t)c;
+    for (int q = 0; q < k; ++q) S = swap(S, __shfl_sync(TD_FULL, inv, q));
+    const int prev = c == 0 ? N - 1 : c - 1;
+    uint32_t last = 0;
+    for (int m = k; m >= 1; --m) {
+        const uint32_t mv = __shfl_sync(TD_FULL, inv, m - 1);
+        const int i = mv & 31, j = (mv >> 5) & 31, kk = (mv >> 10) & 31;
+        if (!(i < j && j < kk && kk < N)) return 0;
+        const uint32_t Xp = __shfl_sync(TD_FULL, X, prev);
+        // the three cut points of s_m^-1 = (i, i + kk - j, kk) in S, found in X
+        // (every lane takes part in every shuffle: they are computed before
+        // the comparisons, never inside a short-circuited condition)
+        const int g0 = i, g1 = i + kk - j, g2 = kk;
+        const uint32_t u0 = __shfl_sync(TD_FULL, S, g0 == 0 ? N - 1 : g0 - 1), v0 = __shfl_sync(TD_FULL, S, g0);
+        const uint32_t u1 = __shfl_sync(TD_FULL, S, g1 - 1), v1 = __shfl_sync(TD_FULL, S, g1);
+        const uint32_t u2 = __shfl_sync(TD_FULL, S, g2 - 1), v2 = __shfl_sync(TD_FULL, S, g2);
+        const bool act = c < N;
+        const uint32_t h0 = __ballot_sync(TD_FULL, act & (Xp == u0) & (X == v0));
+        const uint32_t h1 = __ballot_sync(TD_FULL, act & (Xp == u1) & (X == v1));
+        const uint32_t h2 = __ballot_sync(TD_FULL, act & (Xp == u2) & (X == v2));
+        // each cut is one neighbouring pair, so each mask has one bit; their
+        // union, taken in ascending order, is the move in the caller's array
+        const uint32_t cuts = h0 | h1 | h2;
+        if (__popc(h0) != 1 || __popc(h1) != 1 || __popc(h2) != 1 || __popc(cuts) != 3) return 0;
+        const int a = __ffs(cuts) - 1;
+        const uint32_t rest = cuts & (cuts - 1);
+        const int b = __ffs(rest) - 1;
+        const int e = 31 - __clz(cuts);
+        const uint32_t t = td_pack_move(a, b, e);
+        if (m > 1) {
+            if (c == 0) s.path[k - m] = (uint16_t)t;
+        } else {
+            last = t;
+        }
+        X = swap(X, t);
+        S = swap(S, (uint32_t)i | ((uint32_t)(i + kk - j) << 5) | ((uint32_t)kk << 10));  // S_{m-1} = S_m . s_m^-1
+    }
+    __syncwarp();
+    r.found_move = (uint16_t)last;
+    return 1;
 }
 
 // ---- table of explored states (free order) --------------------------------
@@ -849,6 +959,10 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
     int attempt = 0;     // free order: restarts with another child order (td_attempt_budget)
     uint32_t ord = 0, attempt_exp = 1;
     uint32_t attempt_budget = ORDERED ? ~0u : td_attempt_budget(lim.restart_base, 0);
+    // a unit of a raced instance (the inverse's side, or the instance's side
+    // once it queued the inverse) looks for the other side's verdict every 16
+    // expansions, so that the loser stops soon after the winner
+    bool raced = !ORDERED && dc && dc->side;
     for (;;) {
         if (found >= 0) {
             r.found_move = (uint16_t)found;
@@ -866,6 +980,10 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
                 // held nodes of the abandoned attempt that were not explored to
                 // the end, so it is cleared before its next use
                 ++attempt;
+                // a root search that may race queues its inverse when it starts
+                // attempt dc->race; another warp then searches it alongside
+                if (dc && attempt == dc->race && !dc->side && d0 == 0 && td_spawn_inverse(s, *dc, N))
+                    raced = true;
                 ord = td_order_variant(attempt);
                 attempt_budget = td_attempt_budget(lim.restart_base, attempt);
                 attempt_exp = 1;
@@ -906,6 +1024,16 @@ __device__ td_dfs_out td_dfs(td_warp_smem &s, const uint8_t *lut, const uint32_t
                 // and searching in parallel already varies the order
                 if (hungry > 0 && td_donate(s, *dc, code, d0, level, N, min(hungry, dc->grain)) > 0)
                     attempt_budget = ~0u;
+            }
+        }
+        if constexpr (!ORDERED) {
+            if (raced && (r.expansions & 15u) == 0) {
+                int stop = 0;
+                if (lane == 0) stop = *(volatile int *)&dc->state->found;
+                if (__shfl_sync(TD_FULL, stop, 0)) {
+                    r.status = TD_DFS_ABORTED;
+                    break;
+                }
             }
         }
         if ((r.expansions & 255u) == 0) {

@@ -162,6 +162,10 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
     td_donate_ctx dc;
     dc.ring = 1;
     dc.tickets = 0;
+    dc.side = 0;  // no race in serving
+    dc.race = 0;
+    dc.spawn_base = 0;
+    dc.spawn_capacity = 0;
     dc.deadline_ns = deadline;
     dc.pool = pool;
     dc.items = items;

@@ -121,6 +121,10 @@ def test_configuration_arguments_are_checked(td):
     assert lib.td_configure_restart(0) == td._lib.OK
     assert lib.td_configure_restart(200) == td._lib.OK
     assert lib.td_configure_restart(16) == td._lib.OK  # the default
+    for attempt in (-1, 33):
+        assert lib.td_configure_race(attempt) == INVALID
+    assert lib.td_configure_race(0) == td._lib.OK
+    assert lib.td_configure_race(8) == td._lib.OK  # the default
     for args in ((0, 2, 32), (1, -1, 32), (1, 9, 32), (1, 2, 0)):
         assert lib.td_configure_serve(*args) == INVALID
         assert lib.td_configure_steal(*args) == INVALID

@@ -206,3 +206,66 @@ def test_restart_schedule(emu):
         assert emu.td_emu_order(R, level) == 0
     first_orders = {emu.td_emu_order(a, 0) for a in range(R)}
     assert len(first_orders) == R  # one order per budgeted attempt at the root
+
+
+@pytest.mark.parametrize("seed", [11, 12])
+def test_inverse_instance_gives_the_verdict_and_a_replayable_witness(oracle, emu, seed):
+    """The race of a search against the search of its inverse (td_steal_kernel)
+    rests on three facts, checked here with full sorting on pairs whose array
+    starts anywhere: the inverse instance (td_inverse_pinned, offset 0) has the
+    same odd-cycle count; searching it gives the oracle's verdict on the
+    original pair; and td_witness_from_inverse turns its witness into one that
+    the oracle's replay accepts on the original pair, with the same length."""
+    emu.td_emu_pinned_cycles.argtypes = [C.c_uint64, C.c_int, C.c_int]
+    rng = random.Random(seed)
+    found = 0
+    for _ in range(300):
+        n = rng.randint(2, 12)
+        pi = list(range(n))
+        rng.shuffle(pi)
+        if rng.random() < 0.3:
+            pi = list(range(n))[::-1]
+            for _ in range(rng.randint(0, 2)):
+                a, b = sorted(rng.sample(range(n), 2)) if n > 1 else (0, 0)
+                pi[a], pi[b] = pi[b], pi[a]
+        beta, omega, init = oracle.perm_to_pair(pi)
+        N = n + 1
+        r0 = rng.randrange(N)
+        beta = beta[r0:] + beta[:r0]
+        maxd = rng.randint(1, 7 if n <= 9 else 6)
+        rate = rng.choice([0.0, 0.0, 1.0, 1.5])
+        rc, _, _ = oracle.search(beta, omega, init, rate, maxd, True)
+        x = _prep(emu, beta, omega, init, rate, maxd, True)
+        xi = Inst()
+        emu.td_emu_inverse_instance(C.byref(x), C.byref(xi))
+        assert xi.offset == 0 and xi.packed == x.packed
+        assert emu.td_emu_pinned_cycles(xi.perm, 0, N) == emu.td_emu_pinned_cycles(x.perm, x.offset, N) == init
+        ri, _ = _run(emu, xi, 0)
+        assert ri.status == rc, (pi, r0, maxd, rate)
+        if rc != 1:
+            continue
+        r = Res()
+        assert emu.td_emu_witness_from_inverse(C.byref(x), C.byref(ri), C.byref(r)) == 1
+        assert r.depth == ri.depth and emu.td_emu_witness_ok(C.byref(x), C.byref(r)) == 1
+        moves = [(m & 31, (m >> 5) & 31, (m >> 10) & 31) for m in r.moves[: r.depth]]
+        abc = oracle.positions_to_symbols(beta, moves)
+        assert oracle.validate(beta, omega, abc, maxd) is None, (pi, r0, moves)
+        found += 1
+    assert found > 100
+
+
+def test_inverse_witness_on_s16(oracle, emu):
+    """The same on benchmark-shaped S_16 instances at bound 9 (half
+    near-reverse): every inverse-side witness converts and replays."""
+    perms, n = oracle.synth_perms(7, 64, 16, 16, 50, 1, 4)
+    for p in perms:
+        beta, omega, init = oracle.perm_to_pair(p[:16].tolist())
+        x = _prep(emu, beta, omega, init, 0.0, 9, True)
+        xi = Inst()
+        emu.td_emu_inverse_instance(C.byref(x), C.byref(xi))
+        ri, _ = _run(emu, xi, 0)
+        assert ri.status == 1
+        r = Res()
+        assert emu.td_emu_witness_from_inverse(C.byref(x), C.byref(ri), C.byref(r)) == 1
+        moves = [(m & 31, (m >> 5) & 31, (m >> 10) & 31) for m in r.moves[: r.depth]]
+        assert oracle.validate(beta, omega, oracle.positions_to_symbols(beta, moves), 9) is None

@@ -13,10 +13,12 @@ MiB = 1 << 20
 
 def _library_defaults(td):
     """The engine's own defaults (td_engine.cu): donation grain 4, split level
-    2, idle check every 64 expansions, 4096-entry tables, restart base 16."""
+    2, idle check every 64 expansions, 4096-entry tables, restart base 16, the
+    race against the inverse from restart attempt 8."""
     td._lib.configure_steal(4, 2, 64)
     td._lib.configure_table(12)
     td._lib.configure_restart(16)
+    td._lib.configure_race(8)
 
 
 @pytest.fixture(scope="module")
@@ -352,3 +354,40 @@ def test_batch_stats_match_the_results(slots):
             assert st.errors > 0
     empty, st = td.search_batch(1, inst[:0], 0)
     assert len(empty) == 0 and st.found == st.not_found == st.errors == st.expansions == 0
+
+
+def test_inverse_race_keeps_verdicts_and_witnesses(slots, oracle):
+    """Free-order batches race a search that reaches a given restart attempt
+    against a search of its inverse permutation (td_configure_race).  With and
+    without the race: identical verdicts on hard S_16 at bound 9, on hard
+    n = 13 at bound 6 and on the n = 11..13 mix one below its bound (the last
+    two with many instances that have no witness, where the first side searched
+    to the end decides); the oracle's verdicts on a sample; and every witness,
+    many of them found on the inverse's side and converted, replays on the
+    device (TD_FLAG_VERIFY) and in the oracle."""
+    td = slots
+    p1, n1 = td.synth_perms(3, 2048, 16, 16, 100, 1, 4)
+    p2, n2 = td.synth_perms(5, 2048, 13, 13, 100, 1, 3)
+    p3, n3 = td.synth_perms(1, 4096, 11, 13, 25, 1, 3)
+    sets = [(p1, n1, np.full(len(n1), 9, np.int32)), (p2, n2, np.full(len(n2), 6, np.int32)),
+            (p3, n3, (n3 // 2).astype(np.int32))]
+    try:
+        for perms, n, maxd in sets:
+            inst = td.prepare_perms(perms, n, maxd)
+            td._lib.configure_race(0)
+            plain, st0 = td.search_batch(0, inst, 0)
+            # from the first restart on: the most races, and so the most
+            # witnesses found on the inverse's side
+            td._lib.configure_race(1)
+            raced, st1 = td.search_batch(0, inst, td._lib.FLAG_VERIFY)
+            assert st0.races == 0 and st1.races > 0
+            assert st0.errors == 0 and st1.errors == 0  # a witness failing the device replay would be -6
+            assert (plain["status"] == raced["status"]).all()
+            b, o, init, N = _pairs(oracle, perms[:256], n[:256])
+            ost, _, _, _ = _oracle_batch(oracle, b, o, N, init, 0.0, maxd[:256], 1)
+            assert (raced["status"][:256] == ost).all()
+            b, o, _, N = _pairs(oracle, perms, n)
+            _replay_all(oracle, b, o, N, raced, maxd)
+        assert (plain["status"] == 0).any() and (raced["status"] == 0).sum() == (plain["status"] == 0).sum()
+    finally:
+        _library_defaults(td)
