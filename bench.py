@@ -41,20 +41,22 @@ WORKLOAD = "full-size decision search: 2^20 S_16 perms, 50% uniform / 50% revers
 # Per node expansion at N = 17, the search kernel's warp instructions (all
 # pipes) and those of the integer ALU pipe, and its DRAM bytes per launch: one-
 # pass ncu captures of td_steal_kernel on one launch of this benchmark's 2^20-
-# instance batch with the tuned launch shape, summarised with their commands in
-# profiles/td_steal_kernel_s16_2p20_counters.md.  37.697 G warp instructions
-# and 20.491 G ALU-pipe instructions over the launch's 50.03 M expansions
-# (restarts, skipped children, donation and scheduling included) in
-# 95.96 M SM cycles: the ALU pipe busy 72.1 % of its 2 warp instructions per
-# cycle per SM, issue 66.4 % of 4; 0.901 GB read and 0.834 GB written.
+# instance batch with the tuned launch shape and the race from attempt 8,
+# summarised with their commands in profiles/td_steal_kernel_s16_2p20_counters.md.
+# 37.034 G warp instructions and 20.016 G ALU-pipe instructions over the
+# launch's 48.90 M expansions (restarts, races, skipped children, donation and
+# scheduling included) in 85.75 M SM cycles: the ALU pipe busy 78.9 % of its 2
+# warp instructions per cycle per SM, issue 73.0 % of 4; 0.975 GB read and
+# 0.848 GB written.
 # Free-order searches race the search of their inverse permutation from this
 # restart attempt on (the library's default, td_configure_race).
 RACE_ATTEMPT = 8
-INST_PER_EXPANSION = 37.697e9 / 50.03e6
-ALU_INST_PER_EXPANSION = 20.491e9 / 50.03e6
-ALU_BUSY_MEASURED = 20.491e9 / (95.96e6 * 148 * 2)
-ISSUE_MEASURED = 37.697e9 / (95.96e6 * 148 * 4)
-DRAM_BYTES_PER_LAUNCH = 0.901e9 + 0.834e9
+INST_PER_EXPANSION = 37.034e9 / 48.90e6
+ALU_INST_PER_EXPANSION = 20.016e9 / 48.90e6
+ALU_BUSY_MEASURED = 20.016e9 / (85.75e6 * 148 * 2)
+ISSUE_MEASURED = 37.034e9 / (85.75e6 * 148 * 4)
+DRAM_BYTES_PER_LAUNCH = 0.975e9 + 0.848e9
+
 
 def rank_info():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
