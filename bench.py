@@ -449,6 +449,8 @@ def run_engine(args):
     if not only_engine:
         td.search_batch(0, host_in, _lib.FLAG_VERIFY, out=host_out)  # untimed: sizes the slot's batch buffer
     e2e_ms = []
+    if dist:
+        dist.barrier()
     for k in range(0 if only_engine else args.steps):
         with torch.cuda.stream(stream):
             flush.zero_()
@@ -459,6 +461,11 @@ def run_engine(args):
         e2e_verified += int((res_h["status"] == 1).sum())
     e2e_s = sum(e2e_ms) / 1e3
     e2e_steps = max(1, len(e2e_ms))
+    if dist:
+        # whole job, like `value`: witnesses of every rank over the slowest rank's time
+        from td16_b200 import replicas
+        e2e_s = replicas.max_over_ranks(e2e_s, dist, dev)
+        e2e_verified = int(replicas.sum_over_ranks([e2e_verified], dist, dev)[0])
 
     # the plain one-launch-per-batch form on the same GPU
     plain_ms, plain_verified = float("nan"), 0
@@ -529,8 +536,9 @@ def run_engine(args):
         "nodes_per_s": nodes_per_s, "triples_per_s": triples_per_s,
         "found": found, "not_found": not_found, "errors": errors, "verified": verified,
         "plain_one_launch": {"value": plain_verified / (plain_ms / 1e3), "ms": plain_ms},
-        "e2e": {"value": e2e_verified / e2e_s if e2e_s else None, "unit": UNIT, "h2d_bytes_per_step": count * 16,
-                "d2h_bytes_per_step": count * 32, "ms_per_step": e2e_s / e2e_steps * 1e3, "steps": len(e2e_ms),
+        "e2e": {"value": e2e_verified / e2e_s if e2e_s else None, "unit": UNIT,
+                "h2d_bytes_per_step": count * 16 * world, "d2h_bytes_per_step": count * 32 * world,
+                "ms_per_step": e2e_s / e2e_steps * 1e3, "steps": len(e2e_ms),
                 "ms_min": min(e2e_ms) if e2e_ms else None, "ms_max": max(e2e_ms) if e2e_ms else None},
         "gpu_launches": args.steps * 4,  # per graph replay: epoch, search, finalize, replay
         "launch_shape": {**tuned, "race_from_attempt": RACE_ATTEMPT},
