@@ -160,9 +160,12 @@ int td_configure_restart(int base);
  * its inverse permutation, which another warp runs alongside; the first
  * witness (turned into the instance's positions) or the first side searched
  * to the end decides.  A permutation and its inverse are equally far from
- * sorted, so verdicts do not depend on it.  Default 8; 0 turns the race
- * off.  No counterpart in the reference, whose search runs one order to the
- * end. */
+ * sorted, and a witness found there is kept only if it also keeps the
+ * reference's move filter on the instance's side, so verdicts do not depend
+ * on it.  Default 8; 0 turns the race off.  The per-call server
+ * (td_search), whose warps mostly idle, races from the first restart whenever
+ * the race is on.  No counterpart in the reference, whose search runs one
+ * order to the end. */
 int td_configure_race(int attempt);
 /* Reference-order batches (TD_FLAG_ORDERED, no expansion budget) run every
  * walk on one warp for first_pass_expansions (default 64), then split each

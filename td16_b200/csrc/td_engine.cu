@@ -340,10 +340,12 @@ __global__ void td_split_join_kernel(const int *__restrict__ hard_list, const td
 // wins), and the unit that finishes the search last writes the final status
 // and the summed expansions.  Returns 1 in the warp that finished last.
 // `side` 1 marks a unit of the inverse instance's search (td_steal_kernel's
-// race; its witness is already in the instance's positions).  When the last
-// unit of one side ends with no witness and no error recorded, that side's
-// whole tree was searched: the instance has no witness within the bound, and
-// found = 2 stops the other side.
+// race; its witness is already in the instance's positions and keeps the
+// reference's move filter there).  When the last unit of the instance's own
+// side ends with no witness and no error recorded, its whole filtered tree
+// was searched: the instance has no witness within the bound, and found = 2
+// stops the inverse's side.  The inverse's side never decides "no witness":
+// the filter applies to a different tree there.
 // HOST_OUT: `out` is host memory mapped into the device (the serving loop), so
 // the fences are system-scope; the batch engine's results are device memory,
 // where device-scope fences order the same writes at a fraction of the cost.
@@ -373,8 +375,8 @@ __device__ __forceinline__ int td_finish_unit(const td_dfs_out &r, td_inst_state
         const int before = atomicSub(&st->pending, unit);
         last = before == unit;
         if (last) td_unit_fence<HOST_OUT>();
-        else if (((before - unit) & (side ? 0xffff0000 : 0x0000ffff)) == 0 &&
-                 *(volatile int *)&st->found == 0 && *(volatile int *)&st->error == 0)
+        else if (!side && ((before - unit) & 0x0000ffff) == 0 && *(volatile int *)&st->found == 0 &&
+                 *(volatile int *)&st->error == 0)
             atomicCAS(&st->found, 0, 2);
     }
     last = __shfl_sync(TD_FULL, last, 0);
@@ -609,10 +611,16 @@ __global__ void __launch_bounds__(256, TD_STEAL_MIN_BLOCKS) td_steal_kernel(cons
                     r = td_dfs<false>(s, lut, code, x.n_symbols, x.max_moves, d0, ilim, &dc);
                     dc.side = 0;
                     // a witness of the inverse becomes one of the instance; one that
-                    // does not convert is reported as a failed replay, never recorded
-                    if (side && r.status == TD_DFS_FOUND && !td_inverse_result(s, x, r)) {
-                        r.status = TD_DFS_EXHAUSTED;
-                        if (lane == 0) atomicCAS(&st->error, 0, TD_ERR_VERIFY);
+                    // does not convert is reported as a failed replay, and one that
+                    // leaves the reference's move filter on the instance's side is
+                    // dropped (this side then stops; the instance's own search decides)
+                    if (side && r.status == TD_DFS_FOUND) {
+                        if (!td_inverse_result(s, x, r)) {
+                            r.status = TD_DFS_EXHAUSTED;
+                            if (lane == 0) atomicCAS(&st->error, 0, TD_ERR_VERIFY);
+                        } else if (!td_filtered_witness(s, x, r)) {
+                            r.status = TD_DFS_EXHAUSTED;
+                        }
                     }
                 }
                 td_finish_unit<false>(r, st, &out[idx], s.path, side);

@@ -738,19 +738,57 @@ __device__ __forceinline__ int td_donate(td_warp_smem &s, const td_donate_ctx &d
 // of the race's queue, so that another warp searches it while this one goes
 // on; the first witness on either side ends both, and so does either side
 // searched to the end without one (found = 2).  The pending and outstanding
-// counts cover the item before it can be claimed.  Only an instance's root
-// search queues its inverse, once, and the queue holds a slot per instance of
-// the launch, so one fetch-and-add reserves a slot: busy searches queue their
-// inverses at up to several per microsecond, and a compare-and-swap loop on
-// the counter kept them waiting.  Returns whether it was queued (uniform
-// across the warp).
+// counts cover the item before it can be claimed.  In the batch engine only an
+// instance's root search queues its inverse, once, and the queue holds a slot
+// per instance of the launch, so one fetch-and-add reserves a slot: busy
+// searches queue their inverses at up to several per microsecond, and a
+// compare-and-swap loop on the counter kept them waiting.  In the serving
+// loop (dc.ring) the inverse is one more item of its ring.  Returns whether it
+// was queued (uniform across the warp).
 __device__ __forceinline__ int td_spawn_inverse(const td_warp_smem &s, const td_donate_ctx &dc, int N) {
     int ok = 0;
     if ((threadIdx.x & 31) == 0) {
-        const int slot = atomicAdd(&dc.pool->spawn_produced, 1);
-        if (slot < dc.spawn_capacity) {
-            atomicAdd(&dc.state->pending, 1 << 16);
-            atomicAdd(&dc.pool->outstanding, 1);
+        int slot = -1, phys = -1;
+        uint32_t tag = dc.epoch;
+        if (dc.ring) {
+            // the serving loop's ring of items: reserved like a donation (one
+            // item), and a reused slot is written once its last item was read
+            int cur = *(volatile int *)&dc.pool->produced;
+            for (;;) {
+                if (cur - *(volatile int *)&dc.pool->consumed + 1 > dc.capacity) break;
+                const int prev = atomicCAS(&dc.pool->produced, cur, cur + 1);
+                if (prev == cur) { slot = cur; break; }
+                cur = prev;
+            }
+            if (slot >= 0) {
+                phys = slot % dc.capacity;
+                tag = td_ring_tag(slot);
+                atomicAdd(&dc.state->pending, 1 << 16);
+                if (slot >= dc.capacity) {
+                    const uint32_t freed = td_ring_tag(slot - dc.capacity) | 0x80000000u;
+                    for (unsigned spin = 0; *(volatile uint32_t *)&dc.ready[phys] != freed; ++spin) {
+                        if ((spin & 255u) == 0 && dc.deadline_ns && td_globaltimer() > dc.deadline_ns) {
+                            // the slot still holds an unread item: left alone, and
+                            // this item's taker gives up at the deadline
+                            atomicCAS(&dc.pool->error, 0, TD_ERR_TIMEOUT);
+                            phys = -1;
+                            break;
+                        }
+                        __nanosleep(64);
+                    }
+                }
+            }
+        } else {
+            slot = atomicAdd(&dc.pool->spawn_produced, 1);
+            if (slot < dc.spawn_capacity) {
+                phys = dc.spawn_base + slot;
+                atomicAdd(&dc.state->pending, 1 << 16);
+                atomicAdd(&dc.pool->outstanding, 1);
+            } else {
+                slot = -1;
+            }
+        }
+        if (phys >= 0) {
             td_item it;
             it.L = td_inverse_pinned(s.L[0], N);
             it.inst = dc.inst;
@@ -758,11 +796,11 @@ __device__ __forceinline__ int td_spawn_inverse(const td_warp_smem &s, const td_
             it.off = 0;
 #pragma unroll
             for (int d = 0; d < TD_MAX_DEPTH; ++d) it.path[d] = 0;
-            dc.items[dc.spawn_base + slot] = it;
+            dc.items[phys] = it;
             __threadfence();
-            atomicExch(&dc.ready[dc.spawn_base + slot], dc.epoch);
-            ok = 1;
+            atomicExch(&dc.ready[phys], tag);
         }
+        ok = slot >= 0;
     }
     return __shfl_sync(TD_FULL, ok, 0);
 }
@@ -784,7 +822,7 @@ __device__ __forceinline__ int td_inverse_result(td_warp_smem &s, const td_insta
         if (c >= i && c < kk) src = c < i + (kk - j) ? c + (j - i) : c - (kk - j);
         return __shfl_sync(TD_FULL, v, src);
     };
-    // lane q holds the inverse's move q; the converted moves then go to s.path
+    // lane q holds the inverse's move q, and then the converted move q
     const uint32_t inv = c < k - 1 ? (uint32_t)s.path[c] : (c == k - 1 ? (uint32_t)r.found_move : 0u);
     __syncwarp();
     // X: the caller's array; S: the identity array after all the inverse's moves
@@ -794,7 +832,7 @@ __device__ __forceinline__ int td_inverse_result(td_warp_smem &s, const td_insta
     uint32_t S = (uint32_t)c;
     for (int q = 0; q < k; ++q) S = swap(S, __shfl_sync(TD_FULL, inv, q));
     const int prev = c == 0 ? N - 1 : c - 1;
-    uint32_t last = 0;
+    uint32_t mine = 0;  // lane q: move q of the converted witness
     for (int m = k; m >= 1; --m) {
         const uint32_t mv = __shfl_sync(TD_FULL, inv, m - 1);
         const int i = mv & 31, j = (mv >> 5) & 31, kk = (mv >> 10) & 31;
@@ -820,17 +858,47 @@ __device__ __forceinline__ int td_inverse_result(td_warp_smem &s, const td_insta
         const int b = __ffs(rest) - 1;
         const int e = 31 - __clz(cuts);
         const uint32_t t = td_pack_move(a, b, e);
-        if (m > 1) {
-            if (c == 0) s.path[k - m] = (uint16_t)t;
-        } else {
-            last = t;
-        }
+        if (c == k - m) mine = t;
         X = swap(X, t);
         S = swap(S, (uint32_t)i | ((uint32_t)(i + kk - j) << 5) | ((uint32_t)kk << 10));  // S_{m-1} = S_m . s_m^-1
     }
+    // each lane stores its own move into the path, which it alone read above;
+    // the record's writers read it after the barrier
+    if (c < k - 1) s.path[c] = (uint16_t)mine;
+    r.found_move = (uint16_t)__shfl_sync(TD_FULL, mine, k - 1);
     __syncwarp();
-    r.found_move = (uint16_t)last;
     return 1;
+}
+
+// Whether a witness of instance x (its caller positions: path[0 .. depth-2],
+// found_move) is one the instance's own search could return: every move keeps
+// the reference's move filter (it touches no symbol that omega fixes, and it
+// changes the odd-cycle count by 0 or +2, sorting_search.cu:375-380,
+// 240-332), no node before the last passes the acceptance test, and the last
+// does.  A witness of the inverse, turned into the instance's positions, keeps
+// the filter on the inverse's side but need not on this one: its path passes
+// through other states.  Recording only witnesses that pass keeps the verdict
+// that of the instance's own filtered search.  Uses the warp's frame (levels
+// 0..depth) as scratch; uniform across the warp.
+__device__ __forceinline__ bool td_filtered_witness(td_warp_smem &s, const td_instance &x, const td_dfs_out &r) {
+    const int N = x.n_symbols, k = r.depth;
+    if (k < 1 || k > TD_MAX_DEPTH) return false;
+    td_unpack_state(s, 0, x.perm, x.offset, N);
+    uint32_t O, F;
+    int odd = td_prepare_rows(s, 0, N, O, F);
+    for (int d = 0; d < k; ++d) {
+        const uint32_t t = d == k - 1 ? (uint32_t)r.found_move : (uint32_t)s.path[d];
+        const int i = t & 31, j = (t >> 5) & 31, kk = (t >> 10) & 31;
+        if (!(i < j && j < kk && kk < N)) return false;
+        if (((F >> i) | (F >> j) | (F >> kk)) & 1u) return false;
+        td_apply_bytes(s, d, t, N);
+        const int next = td_prepare_rows(s, d + 1, N, O, F);
+        if (next != odd && next != odd + 2) return false;
+        odd = next;
+        const bool accepted = (s.acc[d + 1] >> odd) & 1u;
+        if (accepted != (d == k - 1)) return false;
+    }
+    return true;
 }
 
 // ---- table of explored states (free order) --------------------------------

@@ -210,7 +210,7 @@ int percall_start(PercallServer &ps, int device, char *err, size_t errlen) {
         ps.d_ring, ps.d_res, ps.d_done, kPercallRing, ps.d_hctl, ps.d_ctl, ps.d_queue, ps.d_state, ps.d_pool,
         ps.d_items, ps.d_ready, kPercallItems, cfg.serve_grain, cfg.serve_split_level, cfg.serve_check_every, 0,
         life_ns, cfg.tt_bits > 0 ? ps.d_tt : nullptr, ps.d_tt_gen, cfg.tt_bits, cfg.restart_base, request_ns,
-        (uint64_t)g_percall_idle_ns.load());
+        (uint64_t)g_percall_idle_ns.load(), cfg.race ? 1 : 0);  // mostly idle warps: race from the first restart
     TD_CHECK(cudaGetLastError());
     ps.grid = grid;
     ps.warps = warps;

@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
                                                       int grain, int max_level, int check_every, uint64_t max_exp,
                                                       uint64_t time_limit_ns, uint64_t *tt, uint32_t *tt_gen,
                                                       int tt_bits, uint32_t restart_base,
-                                                      uint64_t request_limit_ns, uint64_t idle_exit_ns) {
+                                                      uint64_t request_limit_ns, uint64_t idle_exit_ns, int race) {
     constexpr bool ALL_ORDERED = MODE == TD_SERVE_ORDERED;
     extern __shared__ __align__(16) uint8_t td_smem[];
     const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -162,8 +162,8 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
     td_donate_ctx dc;
     dc.ring = 1;
     dc.tickets = 0;
-    dc.side = 0;  // no race in serving
-    dc.race = 0;
+    dc.side = 0;
+    dc.race = 0;  // set per fresh request (the per-call server's race)
     dc.spawn_base = 0;
     dc.spawn_capacity = 0;
     dc.deadline_ns = deadline;
@@ -235,6 +235,7 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
         bool run = false;
         bool ord = ALL_ORDERED;  // this unit's move order (donated subtrees: free)
         int d0 = 0;
+        int side = 0;  // 1: a unit of the request's inverse (the per-call server's race)
         if (kind == 1) {
             const unsigned slot = (unsigned)(req % ring_size);
             const uint4 v = __ldcg(reinterpret_cast<const uint4 *>(&queue[slot]));
@@ -296,7 +297,8 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
                 const uint4 v = __ldcg(reinterpret_cast<const uint4 *>(&queue[slot]));
                 const td_instance x = *reinterpret_cast<const td_instance *>(&v);
                 td_setup_root<false>(s, x, code, codeN);
-                d0 = it.depth;
+                d0 = it.depth & 0x7f;
+                side = it.depth >> 7;
                 if (lane == 0) {
                     s.L[d0] = it.L;
                     s.off[d0] = it.off;
@@ -307,7 +309,7 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
                 if (lane == 0) stop = *(volatile int *)&state[slot].found;
                 run = !__shfl_sync(TD_FULL, stop, 0);
                 if (!run) {  // the request already has its witness
-                    if (td_finish_unit<true>(r, &state[slot], &results[slot], s.path) && lane == 0) {
+                    if (td_finish_unit<true>(r, &state[slot], &results[slot], s.path, side) && lane == 0) {
                         done[slot] = (unsigned long long)req + 1ull;
                         atomicAdd(&dctl->served, 1ull);
                     }
@@ -322,11 +324,29 @@ __global__ void __launch_bounds__(256, 3) td_serve_kernel(const td_instance *rin
             dc.state = &state[slot];
             td_search_limits ulim = lim;
             if (request_limit_ns) ulim.deadline_ns = min(deadline, td_globaltimer() + request_limit_ns);
-            // a fresh request may restart; a donated subtree is searched once
-            ulim.restart_base = kind == 1 ? restart_base : 0;
+            // a fresh request may restart, and so may the root of its inverse; a
+            // donated subtree is searched once.  A fresh free-order request of
+            // the per-call server with full sorting races the search of its
+            // inverse from restart attempt `race` (td_steal_kernel's race).
+            ulim.restart_base = kind == 1 || d0 == 0 ? restart_base : 0;
+            dc.side = side;
+            dc.race = MODE == TD_SERVE_PER_REQUEST && kind == 1 && !ord && restart_base && td_inst_full(x) ? race : 0;
             if (ord) r = td_dfs<true>(s, lut, code, x.n_symbols, x.max_moves, d0, ulim, nullptr);
             else r = td_dfs<false>(s, lut, code, x.n_symbols, x.max_moves, d0, ulim, &dc);
-            if (td_finish_unit<true>(r, &state[slot], &results[slot], s.path) && lane == 0) {
+            dc.side = 0;
+            dc.race = 0;
+            // a witness of the inverse becomes one of the request; one that does
+            // not convert is reported as a failed replay, and one that leaves the
+            // reference's move filter on the request's side is dropped
+            if (side && r.status == TD_DFS_FOUND) {
+                if (!td_inverse_result(s, x, r)) {
+                    r.status = TD_DFS_EXHAUSTED;
+                    if (lane == 0) atomicCAS(&state[slot].error, 0, TD_ERR_VERIFY);
+                } else if (!td_filtered_witness(s, x, r)) {
+                    r.status = TD_DFS_EXHAUSTED;
+                }
+            }
+            if (td_finish_unit<true>(r, &state[slot], &results[slot], s.path, side) && lane == 0) {
                 done[slot] = (unsigned long long)req + 1ull;
                 atomicAdd(&dctl->served, 1ull);
             }
@@ -478,12 +498,12 @@ TD_API int td_serve_open(int device, unsigned ring_size, unsigned flags, double 
         td_serve_kernel<TD_SERVE_ORDERED><<<grid, warps * 32, smem, sv->stream>>>(
             sv->d_ring, sv->d_res, sv->d_done, ring_size, sv->d_hctl, sv->d_ctl, sv->d_queue, sv->d_state,
             sv->d_pool, sv->d_items, sv->d_ready, sv->item_capacity, cfg.serve_grain, cfg.serve_split_level,
-            cfg.serve_check_every, 0, limit_ns, nullptr, nullptr, 0, 0u, 0ull, 0ull);
+            cfg.serve_check_every, 0, limit_ns, nullptr, nullptr, 0, 0u, 0ull, 0ull, 0);
     else
         td_serve_kernel<TD_SERVE_FREE><<<grid, warps * 32, smem, sv->stream>>>(
             sv->d_ring, sv->d_res, sv->d_done, ring_size, sv->d_hctl, sv->d_ctl, sv->d_queue, sv->d_state,
             sv->d_pool, sv->d_items, sv->d_ready, sv->item_capacity, cfg.serve_grain, cfg.serve_split_level,
-            cfg.serve_check_every, 0, limit_ns, sv->d_tt, sv->d_tt_gen, tt_bits, 0u, 0ull, 0ull);
+            cfg.serve_check_every, 0, limit_ns, sv->d_tt, sv->d_tt_gen, tt_bits, 0u, 0ull, 0ull, 0);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, __LINE__);
     *handle = sv;
     return TD_OK;

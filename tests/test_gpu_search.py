@@ -50,13 +50,37 @@ def _oracle_batch(oracle, beta, omega, N, init, rate, maxd, full):
                                np.broadcast_to(full, (c,)).astype(np.uint8), os.cpu_count() or 8)
 
 
+def _keeps_filter(oracle, beta, omega, moves):
+    """Every move keeps the reference's move filter: it touches no symbol that
+    omega fixes and changes the odd-cycle count by 0 or +2
+    (sorting_search.cu:240-332, 375-380)."""
+    beta, omega = list(beta), list(omega)
+    odd = oracle.count_odd_cycles(omega)
+    for (i, j, k) in moves:
+        a, b, c = beta[i], beta[j], beta[k]
+        if omega[a] == a or omega[b] == b or omega[c] == c:
+            return False
+        nxt = list(omega)
+        nxt[a], nxt[b], nxt[c] = omega[c], omega[a], omega[b]
+        d = oracle.count_odd_cycles(nxt) - odd
+        if d not in (0, 2):
+            return False
+        odd += d
+        omega = nxt
+        beta = beta[:i] + beta[j:k] + beta[i:j] + beta[k:]
+    return True
+
+
 def _replay_all(oracle, beta, omega, N, res, maxd):
+    """Every witness replays in the checker and keeps the reference's move
+    filter (witnesses found on an inverse's side included)."""
     for i in np.nonzero(res["status"] == 1)[0]:
         k = int(N[i])
         moves = [(int(m) & 31, (int(m) >> 5) & 31, (int(m) >> 10) & 31) for m in res["moves"][i][: res["depth"][i]]]
         abc = oracle.positions_to_symbols(beta[i, :k].tolist(), moves)
         err = oracle.validate(beta[i, :k].tolist(), omega[i, :k].tolist(), abc, int(np.broadcast_to(maxd, (len(N),))[i]))
         assert err is None, (i, err)
+        assert _keeps_filter(oracle, beta[i, :k].tolist(), omega[i, :k].tolist(), moves), (i, moves)
 
 
 def test_smoke_concurrent_three_cycles_through_the_slot_queue(td):
@@ -361,10 +385,12 @@ def test_inverse_race_keeps_verdicts_and_witnesses(slots, oracle):
     against a search of its inverse permutation (td_configure_race).  With and
     without the race: identical verdicts on hard S_16 at bound 9, on hard
     n = 13 at bound 6 and on the n = 11..13 mix one below its bound (the last
-    two with many instances that have no witness, where the first side searched
-    to the end decides); the oracle's verdicts on a sample; and every witness,
+    two with many instances that have no witness, which the instance's own
+    search decides); the oracle's verdicts on a sample; and every witness,
     many of them found on the inverse's side and converted, replays on the
-    device (TD_FLAG_VERIFY) and in the oracle."""
+    device (TD_FLAG_VERIFY) and in the oracle and keeps the reference's move
+    filter (a converted witness that leaves it is dropped, and the instance's
+    own search decides)."""
     td = slots
     p1, n1 = td.synth_perms(3, 2048, 16, 16, 100, 1, 4)
     p2, n2 = td.synth_perms(5, 2048, 13, 13, 100, 1, 3)
