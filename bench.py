@@ -43,20 +43,20 @@ WORKLOAD = "full-size decision search: 2^20 S_16 perms, 50% uniform / 50% revers
 # pass ncu captures of td_steal_kernel on one launch of this benchmark's 2^20-
 # instance batch with the tuned launch shape and the race from attempt 8,
 # summarised with their commands in profiles/td_steal_kernel_s16_2p20_counters.md.
-# 37.034 G warp instructions and 20.016 G ALU-pipe instructions over the
-# launch's 48.90 M expansions (restarts, races, skipped children, donation and
-# scheduling included) in 85.75 M SM cycles: the ALU pipe busy 78.9 % of its 2
-# warp instructions per cycle per SM, issue 73.0 % of 4; 0.975 GB read and
-# 0.848 GB written.
+# 36.870 G warp instructions and 19.901 G ALU-pipe instructions over the
+# launch's 49.02 M expansions (restarts, races, skipped children, donation and
+# scheduling included) in 85.21 M SM cycles: the ALU pipe busy 78.9 % of its 2
+# warp instructions per cycle per SM, issue 73.1 % of 4; 0.963 GB read and
+# 0.840 GB written.
 # Free-order searches race the search of their inverse permutation from this
 # restart attempt on (the library's default, td_configure_race).
 RACE_ATTEMPT = 8
 PLAIN_WARPS = 4  # block shape of the plain one-launch-per-batch leg
-INST_PER_EXPANSION = 37.034e9 / 48.90e6
-ALU_INST_PER_EXPANSION = 20.016e9 / 48.90e6
-ALU_BUSY_MEASURED = 20.016e9 / (85.75e6 * 148 * 2)
-ISSUE_MEASURED = 37.034e9 / (85.75e6 * 148 * 4)
-DRAM_BYTES_PER_LAUNCH = 0.975e9 + 0.848e9
+INST_PER_EXPANSION = 36.870e9 / 49.02e6
+ALU_INST_PER_EXPANSION = 19.901e9 / 49.02e6
+ALU_BUSY_MEASURED = 19.901e9 / (85.21e6 * 148 * 2)
+ISSUE_MEASURED = 36.870e9 / (85.21e6 * 148 * 4)
+DRAM_BYTES_PER_LAUNCH = 0.963e9 + 0.840e9
 
 
 def rank_info():
