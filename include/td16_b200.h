@@ -395,7 +395,7 @@ int td_replay_symbols_device(int count, const uint8_t *d_beta, const uint8_t *d_
 
 /* Batched certificate sink with AsyncCertificateWriter's queue-and-flush
  * behaviour (AsyncCertificateWriter.java:50-116), writing flat records
- * [key_len][value_len][key][value] (RocksDB is not part of this build). */
+ * [key_len][value_len][key][value] (RocksDB is not linked into this library). */
 void *td_cert_writer_open(const char *path, double flush_seconds);
 int td_cert_writer_enqueue(void *writer, const uint8_t *omega, int n,
                            const uint8_t *abc, int count);
