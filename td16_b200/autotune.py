@@ -9,7 +9,9 @@ launch on a sample for every point of a grid over
 and then, with the winning shape, the restart budget base of the root searches
 (0 = no restarts); when restarts win, the grid is searched again with that
 base and the base swept once more, since restarts shorten the searches that
-the donation knobs were tuned for.  The fastest point by device time is kept,
+the donation knobs were tuned for, and last the restart attempt from which a
+search races the search of its inverse permutation (0 = no race; the race
+needs restarts).  The fastest point by device time is kept,
 and the winners per bucket are stored in td16_b200/tuned.json.  `apply(N)`
 configures the engine for a bucket.
 
@@ -28,7 +30,8 @@ import numpy as np
 from . import _lib
 
 TUNED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned.json")
-DEFAULT = {"warps": 4, "grain": 4, "split_level": 2, "check_every": 64, "restart": 16}  # the library's defaults
+DEFAULT = {"warps": 4, "grain": 4, "split_level": 2, "check_every": 64, "restart": 16,
+           "race": 8}  # the library's defaults
 
 GRID = {
     "warps": [4, 8],
@@ -40,12 +43,14 @@ QUICK = {"warps": [2, 4], "grain": [4, 8], "split_level": [4], "check_every": [3
 
 
 RESTARTS = [0, 16, 24, 32, 48, 64, 128]
+RACES = [0, 4, 8, 16]  # restart attempt from which a search races its inverse; 0 = no race
 
 
 def _configure(p):
     _lib.configure(p["warps"], 1)
     _lib.configure_steal(p["grain"], p["split_level"], p["check_every"])
     _lib.configure_restart(p.get("restart", 0))
+    _lib.configure_race(p.get("race", DEFAULT["race"]))
 
 
 def time_point(slot: int, instances: np.ndarray, params: dict, repeats: int = 2) -> float:
@@ -84,10 +89,21 @@ def tune_bucket(slot: int, instances: np.ndarray, grid=None, repeats: int = 2, l
                 best_ms, best = ms, p
         return best_ms, best
 
+    def races(best_ms, best):
+        for attempt in RACES:
+            p = dict(best, race=attempt)
+            ms = time_point(slot, instances, p, repeats)
+            results.append((ms, p))
+            log(f"  {p} -> {ms:.2f} ms")
+            if ms < best_ms:
+                best_ms, best = ms, p
+        return best_ms, best
+
     best_ms, best = bases(*shapes(0))
     if best["restart"]:
         best_ms, best = min([(best_ms, best), shapes(best["restart"])], key=lambda r: r[0])
         best_ms, best = bases(best_ms, best)
+        best_ms, best = races(best_ms, best)
     _configure(DEFAULT)
     return {"params": best, "kernel_ms": best_ms, "points": len(results)}
 
