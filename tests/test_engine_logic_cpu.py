@@ -269,3 +269,49 @@ def test_inverse_witness_on_s16(oracle, emu):
         assert emu.td_emu_witness_from_inverse(C.byref(x), C.byref(ri), C.byref(r)) == 1
         moves = [(m & 31, (m >> 5) & 31, (m >> 10) & 31) for m in r.moves[: r.depth]]
         assert oracle.validate(beta, omega, oracle.positions_to_symbols(beta, moves), 9) is None
+
+
+def _keeps_move_filter(oracle, beta, omega, moves):
+    """The reference's move filter along a witness: no move touches a symbol
+    that omega fixes, and each changes the odd-cycle count by 0 or +2
+    (sorting_search.cu:240-332, 375-380)."""
+    beta, omega = list(beta), list(omega)
+    odd = oracle.count_odd_cycles(omega)
+    for (i, j, k) in moves:
+        a, b, c = beta[i], beta[j], beta[k]
+        if omega[a] == a or omega[b] == b or omega[c] == c:
+            return False
+        nxt = list(omega)
+        nxt[a], nxt[b], nxt[c] = omega[c], omega[a], omega[b]
+        d = oracle.count_odd_cycles(nxt) - odd
+        if d not in (0, 2):
+            return False
+        odd += d
+        omega = nxt
+        beta = beta[:i] + beta[j:k] + beta[i:j] + beta[k:]
+    return True
+
+
+def test_converted_witnesses_replay_but_may_leave_the_move_filter(oracle, emu):
+    """Why the race checks every converted witness against the move filter on
+    the instance's side (td_filtered_witness) before recording it: on
+    near-reverse S_16 at bound 9, every witness of the inverse instance,
+    converted, replays in the checker, yet some take a -2 move or touch a
+    fixed symbol, which the reference's search never does.  The engine's own
+    free-order witnesses always keep the filter."""
+    perms, n = oracle.synth_perms(2, 600, 16, 16, 100, 1, 4)
+    left = 0
+    for p in perms:
+        beta, omega, init = oracle.perm_to_pair(p[:16].tolist())
+        x = _prep(emu, beta, omega, init, 0.0, 9, True)
+        r0, own = _run(emu, x, 0)
+        assert r0.status == 1 and _keeps_move_filter(oracle, beta, omega, own)
+        xi = Inst()
+        emu.td_emu_inverse_instance(C.byref(x), C.byref(xi))
+        ri, _ = _run(emu, xi, 0)
+        r = Res()
+        assert emu.td_emu_witness_from_inverse(C.byref(x), C.byref(ri), C.byref(r)) == 1
+        moves = [(m & 31, (m >> 5) & 31, (m >> 10) & 31) for m in r.moves[: r.depth]]
+        assert oracle.validate(beta, omega, oracle.positions_to_symbols(beta, moves), 9) is None
+        left += not _keeps_move_filter(oracle, beta, omega, moves)
+    assert 0 < left < len(perms) // 10
